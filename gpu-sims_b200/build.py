@@ -1,0 +1,82 @@
+"""Builds liblbm_b200.so (CUDA sm_100a kernels + C++ host runtime) in-tree.
+
+    python gpu-sims_b200/build.py [--force]
+
+Objects go to gpu-sims_b200/_build/, the library to gpu-sims_b200/lbm/.
+nvcc cross-compiles for sm_100a without a GPU.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+CSRC = PKG / "csrc"
+BUILD = PKG / "_build"
+OUT = PKG / "lbm" / "liblbm_b200.so"
+INCLUDE = PKG.parent / "include"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+CUDA_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr",
+              "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+              "-I", str(INCLUDE)] + ARCH
+# The voxeliser must round every float op like the reference's host C++.
+HOST_EXTRA = {"host_tools.cpp": ["-Xcompiler", "-ffp-contract=off"]}
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def sources() -> list[Path]:
+    return sorted(list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cpp")))
+
+
+def _stale(obj: Path, src: Path) -> bool:
+    if not obj.exists():
+        return True
+    deps = [src] + list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
+    return any(d.stat().st_mtime > obj.stat().st_mtime for d in deps)
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    BUILD.mkdir(exist_ok=True)
+    cc = nvcc()
+    objs = []
+    for src in sources():
+        obj = BUILD / (src.name + ".o")
+        objs.append(obj)
+        if not force and not _stale(obj, src):
+            continue
+        cmd = [cc, "-c", str(src), "-o", str(obj)] + CUDA_FLAGS + HOST_EXTRA.get(src.name, [])
+        if src.suffix == ".cpp":
+            cmd = [cc, "-x", "cu", "-c", str(src), "-o", str(obj)] + CUDA_FLAGS + HOST_EXTRA.get(src.name, [])
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    if force or not OUT.exists() or any(o.stat().st_mtime > OUT.stat().st_mtime for o in objs):
+        cmd = [cc, "-shared", "-o", str(OUT)] + [str(o) for o in objs] + ARCH
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return OUT
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("-v", "--verbose", action="store_true")
+    a = ap.parse_args()
+    print(build(force=a.force, verbose=a.verbose))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,108 @@
+// Internal declarations shared by the host runtime and the kernel files.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include "../../include/lbm.h"
+
+namespace lbm {
+
+// Launch-time parameters of the reference-mode (two-buffer) kernels.
+struct RefParams {
+  int nx, ny, nz;
+  size_t n;            // nx*ny*nz; stride between direction planes
+  float tau_inv;       // 1.0f / tau          (src/main.cpp:1525)
+  float omtau_inv;     // 1.0f - tau_inv      (src/main.cpp:1526)
+  float u_inf[3];
+  float rho0;
+  int inlet_outlet;
+  int free_slip;
+  int u_round;         // enum lbm_u_round
+};
+
+// Geometry of the padded esoteric-pull population store (physics mode).
+// Slot arrays: 0 = rest; pair p owns arrays 1+2p and 2+2p.  Node (x,y,z)
+// lives at  x + px*((y+gy) + py*(z+gz));  non-periodic axes carry one ghost
+// layer (x: only at x = nx, since every pair's forward vector has cx >= 0).
+struct PhysGeom {
+  int nx, ny, nz;
+  int px, py, pz;      // padded extents
+  int gy, gz;          // ghost offsets (0 or 1)
+  int per[3];          // periodic flags
+  size_t n;            // natural node count
+  size_t slot_stride;  // elements per slot array
+};
+
+struct PhysParams {
+  PhysGeom g;
+  float omega;         // 1/tau
+  float tau;
+  float trt_magic;
+  float smag_cs;
+  float accel[3];
+  float wall[6][3];
+  int any_moving_wall;
+};
+
+struct Ctx;
+
+// reference-mode kernels (ref_kernels.cu)
+cudaError_t ref_init(const Ctx& c, const float* rho, const float* u3, float rho0,
+                     const float* u0, cudaStream_t s);
+cudaError_t ref_step(const Ctx& c, const float* fin, float* fout, bool write_moments,
+                     cudaStream_t s);
+
+// physics-mode kernels (phys_kernels.cu)
+cudaError_t phys_init(const Ctx& c, const float* rho, const float* u3, float rho0,
+                      const float* u0, cudaStream_t s);
+cudaError_t phys_step(const Ctx& c, int parity, bool write_moments, cudaStream_t s);
+cudaError_t phys_read_pops(const Ctx& c, float* out, cudaStream_t s);
+cudaError_t phys_write_pops(const Ctx& c, const float* in, cudaStream_t s);
+
+// shared utilities (util_kernels.cu)
+cudaError_t classify(const Ctx& c, const int per[3], cudaStream_t s);
+int cons_blocks(size_t n);
+cudaError_t conservation_partials(const Ctx& c, cudaStream_t s);
+cudaError_t u_planes_to_format(const float* u, size_t n, int fmt, void* out, cudaStream_t s);
+cudaError_t u_format_to_planes(const void* in, size_t n, int fmt, float* u, cudaStream_t s);
+
+struct Ctx {
+  lbm_desc d{};
+  int device = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  size_t n = 0;
+  // reference mode: two full population buffers, natural layout [19][n]
+  float* fbuf[2] = {nullptr, nullptr};
+  int cur = 0;
+  RefParams rp{};
+  // physics mode: one esoteric-pull store
+  void* pop = nullptr;
+  int parity = 0;
+  PhysParams pp{};
+  // shared
+  uint8_t* mask = nullptr;    // raw mask as uploaded
+  uint8_t* flags = nullptr;   // classification byte
+  uint32_t* links = nullptr;  // classification word
+  float* rho = nullptr;       // [n]
+  float* u = nullptr;         // [3][n]
+  unsigned* status = nullptr; // device status word
+  double* partials = nullptr; // conservation block partials [4][nblk]
+  double* sums = nullptr;     // [4]
+  int nblk_cons = 0;
+  void* staging = nullptr;    // device staging for host format conversion
+  size_t staging_bytes = 0;
+  bool initialized = false;
+  uint64_t iteration = 0;
+  uint64_t dev_bytes = 0;
+  std::string err;
+};
+
+size_t elem_bytes(int precision);
+double bytes_per_node(const lbm_desc& d);
+
+}  // namespace lbm
+
+struct lbm_ctx : lbm::Ctx {};

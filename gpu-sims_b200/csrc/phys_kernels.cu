@@ -1,0 +1,489 @@
+// Physics-mode kernels: one fused stream+collide launch per step on a single
+// in-place population store (esoteric pull).
+//
+// Layout.  Each opposite pair (a, b = opp a) with forward vector d = c_a owns
+// two slot arrays S0, S1; the rest population owns one.  A launch of parity P
+// touches, for node n, exactly two slots of each pair,
+//     X = S[1-P](n)      and      Y = S[P](n + d),
+// reads the streamed-in f_a from X and f_b from Y, and writes the new
+// post-collision f*_b to X and f*_a to Y.  Between launches this means
+//     before parity 0:  S0(m) = f*_b(m),      S1(m) = f*_a(m - d)
+//     before parity 1:  S0(m) = f*_a(m - d),  S1(m) = f*_b(m)
+// so every launch streams and collides with no second buffer and no two
+// threads touching one slot.
+//
+// Half-way bounce-back.  If n + d is a wall, f_b(n) arrives as the f*_a(n)
+// that n itself wrote at the previous launch, which sits in the other slot of
+// the same location: S[1-P](n + d).  If n - d is a wall, f_a(n) arrives as
+// f*_b(n) from S[P](n).  Nobody else touches those slots (the node beyond is
+// a solid that never runs, or a ghost).  Non-periodic faces therefore carry
+// one ghost layer; periodic axes wrap.  Moving walls add the momentum term
+// 6 w_i rho_w (c_i . u_w), rho_w = 1.
+//
+// Populations are stored shifted, g_i = f_i - w_i, in fp32, fp16 (scaled by
+// 2^12) or bf16; all arithmetic is fp32.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "d3q19.cuh"
+#include "lbm_internal.h"
+
+namespace lbm {
+
+constexpr float F16_SCALE = 4096.0f;
+constexpr float F16_INV_SCALE = 1.0f / 4096.0f;
+
+template <int PREC> struct Store;
+template <> struct Store<LBM_PREC_F32> {
+  using T = float;
+  static __device__ __forceinline__ float ld(const T* p, size_t i) { return p[i]; }
+  static __device__ __forceinline__ void st(T* p, size_t i, float v) { p[i] = v; }
+};
+template <> struct Store<LBM_PREC_F16S> {
+  using T = __half;
+  static __device__ __forceinline__ float ld(const T* p, size_t i) {
+    return __half2float(p[i]) * F16_INV_SCALE;
+  }
+  static __device__ __forceinline__ void st(T* p, size_t i, float v) {
+    p[i] = __float2half_rn(v * F16_SCALE);
+  }
+};
+template <> struct Store<LBM_PREC_BF16S> {
+  using T = __nv_bfloat16;
+  static __device__ __forceinline__ float ld(const T* p, size_t i) { return __bfloat162float(p[i]); }
+  static __device__ __forceinline__ void st(T* p, size_t i, float v) { p[i] = __float2bfloat16_rn(v); }
+};
+
+namespace {
+
+__device__ __forceinline__ size_t lin(const PhysGeom& g, int x, int y, int z) {
+  return (size_t)x + (size_t)g.px * ((size_t)(y + g.gy) + (size_t)g.py * (size_t)(z + g.gz));
+}
+
+// Padded index of n + d: periodic axes wrap, others step into the ghost layer.
+template <int DX, int DY, int DZ>
+__device__ __forceinline__ size_t lin_fwd(const PhysGeom& g, int x, int y, int z) {
+  int xn = x + DX, yn = y + DY, zn = z + DZ;
+  if (DX != 0 && g.per[0]) xn = xn >= g.nx ? xn - g.nx : xn;
+  if (DY != 0 && g.per[1]) yn = yn >= g.ny ? yn - g.ny : (yn < 0 ? yn + g.ny : yn);
+  if (DZ != 0 && g.per[2]) zn = zn >= g.nz ? zn - g.nz : (zn < 0 ? zn + g.nz : zn);
+  return lin(g, xn, yn, zn);
+}
+
+// Moving-wall term for the population arriving in direction J after
+// reflecting off the wall crossed by the link n -> n + c_opp(J).  A link that
+// leaves the box through a z face takes that face's velocity, then y, then x
+// (so lid edges move with the lid); a link into an interior solid sees a
+// resting wall.
+template <int J>
+__device__ __forceinline__ float wall_term(const PhysParams& p, int x, int y, int z) {
+  constexpr int K = opp(J);
+  const int tx = x + cx(K), ty = y + cy(K), tz = z + cz(K);
+  const PhysGeom& g = p.g;
+  int face = -1;
+  if (!g.per[2] && (tz < 0 || tz >= g.nz)) face = tz < 0 ? LBM_FACE_ZM : LBM_FACE_ZP;
+  else if (!g.per[1] && (ty < 0 || ty >= g.ny)) face = ty < 0 ? LBM_FACE_YM : LBM_FACE_YP;
+  else if (!g.per[0] && (tx < 0 || tx >= g.nx)) face = tx < 0 ? LBM_FACE_XM : LBM_FACE_XP;
+  if (face < 0) return 0.0f;
+  const float cu = cx(J) * p.wall[face][0] + cy(J) * p.wall[face][1] + cz(J) * p.wall[face][2];
+  return 6.0f * wf(J) * cu;
+}
+
+// Collision on shifted populations g = f - w, in place.  Returns the moments
+// (rho and the force-shifted velocity) for readback.
+template <int COLL, bool SMAG, bool FORCE>
+__device__ __forceinline__ void collide(const PhysParams& p, float (&g)[Q], float& rho_out,
+                                        float& ux, float& uy, float& uz) {
+  float drho = 0.0f, jx = 0.0f, jy = 0.0f, jz = 0.0f;
+  static_for<0, Q>([&](auto I) {
+    constexpr int i = decltype(I)::value;
+    drho += g[i];
+    if (cx(i)) jx += cx(i) * g[i];
+    if (cy(i)) jy += cy(i) * g[i];
+    if (cz(i)) jz += cz(i) * g[i];
+  });
+  const float rho = 1.0f + drho;
+  const float irho = 1.0f / rho;
+  ux = jx * irho;
+  uy = jy * irho;
+  uz = jz * irho;
+  float Fx = 0.f, Fy = 0.f, Fz = 0.f;
+  if (FORCE) {
+    Fx = rho * p.accel[0];
+    Fy = rho * p.accel[1];
+    Fz = rho * p.accel[2];
+    ux += 0.5f * p.accel[0];
+    uy += 0.5f * p.accel[1];
+    uz += 0.5f * p.accel[2];
+  }
+  rho_out = rho;
+  const float uu15 = 1.5f * (ux * ux + uy * uy + uz * uz);
+
+  float omega = p.omega;
+  if (SMAG) {
+    // Non-equilibrium momentum flux Pi = sum c c (f - feq) and the
+    // Hou et al. (1996) effective relaxation time
+    //   tau_eff = (tau + sqrt(tau^2 + 18 sqrt(2) Cs^2 |Pi| / rho)) / 2.
+    float pxx = 0.f, pyy = 0.f, pzz = 0.f, pxy = 0.f, pxz = 0.f, pyz = 0.f;
+    static_for<0, Q>([&](auto I) {
+      constexpr int i = decltype(I)::value;
+      const float cu = cx(i) * ux + cy(i) * uy + cz(i) * uz;
+      const float geq = wf(i) * (drho + rho * (3.0f * cu + 4.5f * cu * cu - uu15));
+      const float ne = g[i] - geq;
+      if (cx(i)) pxx += ne;
+      if (cy(i)) pyy += ne;
+      if (cz(i)) pzz += ne;
+      if (cx(i) * cy(i)) pxy += cx(i) * cy(i) * ne;
+      if (cx(i) * cz(i)) pxz += cx(i) * cz(i) * ne;
+      if (cy(i) * cz(i)) pyz += cy(i) * cz(i) * ne;
+    });
+    const float pn = sqrtf(pxx * pxx + pyy * pyy + pzz * pzz +
+                           2.0f * (pxy * pxy + pxz * pxz + pyz * pyz));
+    const float cs2 = p.smag_cs * p.smag_cs;
+    const float tau_eff = 0.5f * (p.tau + sqrtf(p.tau * p.tau + 25.455844f * cs2 * pn * irho));
+    omega = 1.0f / tau_eff;
+  }
+
+  if (COLL == LBM_COLL_BGK) {
+    const float fpre = 1.0f - 0.5f * omega;
+    static_for<0, Q>([&](auto I) {
+      constexpr int i = decltype(I)::value;
+      const float cu = cx(i) * ux + cy(i) * uy + cz(i) * uz;
+      const float geq = wf(i) * (drho + rho * (3.0f * cu + 4.5f * cu * cu - uu15));
+      float gn = g[i] + omega * (geq - g[i]);
+      if (FORCE) {
+        const float cF = cx(i) * Fx + cy(i) * Fy + cz(i) * Fz;
+        const float uF = ux * Fx + uy * Fy + uz * Fz;
+        gn += fpre * wf(i) * (3.0f * (cF - uF) + 9.0f * cu * cF);
+      }
+      g[i] = gn;
+    });
+  } else {
+    // TRT: omega+ = omega, omega- from the magic parameter
+    //   Lambda = (1/omega+ - 1/2)(1/omega- - 1/2).
+    const float tau_p = 1.0f / omega;
+    const float omega_m = 1.0f / (p.trt_magic / (tau_p - 0.5f) + 0.5f);
+    const float fp = 1.0f - 0.5f * omega, fm = 1.0f - 0.5f * omega_m;
+    const float uF = FORCE ? (ux * Fx + uy * Fy + uz * Fz) : 0.0f;
+    {
+      const float geq0 = wf(0) * (drho - rho * uu15);
+      float g0 = g[0] + omega * (geq0 - g[0]);
+      if (FORCE) g0 += fp * wf(0) * (-3.0f * uF);
+      g[0] = g0;
+    }
+    static_for<0, 9>([&](auto P) {
+      constexpr int a = pair_a(decltype(P)::value), b = pair_b(decltype(P)::value);
+      const float cu = cx(a) * ux + cy(a) * uy + cz(a) * uz;
+      const float eqp = wf(a) * (drho + rho * (4.5f * cu * cu - uu15));
+      const float eqm = wf(a) * rho * 3.0f * cu;
+      const float gp = 0.5f * (g[a] + g[b]), gm = 0.5f * (g[a] - g[b]);
+      const float dp = omega * (eqp - gp), dm = omega_m * (eqm - gm);
+      float na = g[a] + dp + dm, nb = g[b] + dp - dm;
+      if (FORCE) {
+        const float cF = cx(a) * Fx + cy(a) * Fy + cz(a) * Fz;
+        const float sp = fp * wf(a) * (-3.0f * uF + 9.0f * cu * cF);
+        const float sm = fm * wf(a) * 3.0f * cF;
+        na += sp + sm;
+        nb += sp - sm;
+      }
+      g[a] = na;
+      g[b] = nb;
+    });
+  }
+}
+
+template <int PREC, int COLL, bool SMAG, bool FORCE, bool WRITE_MOMENTS>
+__global__ void __launch_bounds__(256)
+    k_phys_step(PhysParams p, int P, void* __restrict__ pop_v, const uint8_t* __restrict__ flags,
+                const uint32_t* __restrict__ links, float* __restrict__ rho_o,
+                float* __restrict__ u_o, unsigned* __restrict__ status) {
+  using S = Store<PREC>;
+  using T = typename S::T;
+  const PhysGeom& G = p.g;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z * blockDim.z + threadIdx.z;
+  if (x >= G.nx || y >= G.ny || z >= G.nz) return;
+  const size_t N = G.n;
+  const size_t nid = (size_t)x + (size_t)G.nx * ((size_t)y + (size_t)G.ny * (size_t)z);
+  const uint8_t fl = flags[nid];
+  if (fl & FLAG_SOLID) {
+    if (WRITE_MOMENTS) {
+      rho_o[nid] = 0.0f;
+      u_o[nid] = 0.0f;
+      u_o[N + nid] = 0.0f;
+      u_o[2 * N + nid] = 0.0f;
+    }
+    return;
+  }
+  T* pop = reinterpret_cast<T*>(pop_v);
+  const size_t SS = G.slot_stride;
+  const size_t ln = lin(G, x, y, z);
+  const uint32_t L = (fl & FLAG_BOUNDARY) ? links[nid] : 0u;
+  const bool moving = p.any_moving_wall && L;
+
+  float g[Q];
+  size_t lf[9];
+  g[0] = S::ld(pop, ln);
+  static_for<0, 9>([&](auto PI) {
+    constexpr int pi = decltype(PI)::value;
+    constexpr int a = pair_a(pi), b = pair_b(pi);
+    const size_t fwd = lin_fwd<cx(a), cy(a), cz(a)>(G, x, y, z);
+    lf[pi] = fwd;
+    const T* s0 = pop + (size_t)(1 + 2 * pi) * SS;
+    const T* s1 = s0 + SS;
+    const T* sP = P ? s1 : s0;   // S[P]
+    const T* sQ = P ? s0 : s1;   // S[1-P]
+    if (!L) {
+      g[a] = S::ld(sQ, ln);
+      g[b] = S::ld(sP, fwd);
+    } else {
+      const bool blk_fwd = (L >> a) & 1u;  // n + d is a wall
+      const bool blk_bwd = (L >> b) & 1u;  // n - d is a wall
+      g[a] = blk_bwd ? S::ld(sP, ln) : S::ld(sQ, ln);
+      g[b] = blk_fwd ? S::ld(sQ, fwd) : S::ld(sP, fwd);
+      if (moving) {
+        if (blk_bwd) g[a] += wall_term<a>(p, x, y, z);
+        if (blk_fwd) g[b] += wall_term<b>(p, x, y, z);
+      }
+    }
+  });
+
+  float rho, ux, uy, uz;
+  collide<COLL, SMAG, FORCE>(p, g, rho, ux, uy, uz);
+
+  if (WRITE_MOMENTS) {
+    rho_o[nid] = rho;
+    u_o[nid] = ux;
+    u_o[N + nid] = uy;
+    u_o[2 * N + nid] = uz;
+    if (!(rho > 0.0f) || !isfinite(rho) || !isfinite(ux) || !isfinite(uy) || !isfinite(uz))
+      atomicOr(status, 1u);
+  }
+
+  S::st(pop, ln, g[0]);
+  static_for<0, 9>([&](auto PI) {
+    constexpr int pi = decltype(PI)::value;
+    constexpr int a = pair_a(pi), b = pair_b(pi);
+    T* s0 = pop + (size_t)(1 + 2 * pi) * SS;
+    T* s1 = s0 + SS;
+    S::st(P ? s1 : s0, lf[pi], g[a]);  // f*_a -> Y = S[P](n + d)
+    S::st(P ? s0 : s1, ln, g[b]);      // f*_b -> X = S[1-P](n)
+  });
+}
+
+// Places post-collision populations (shifted) of node n where the next
+// launch of parity P expects them: f*_a(n) -> S[1-P](n + d), f*_b(n) ->
+// S[P](n), rest -> R(n).  Used by init and by lbm_write_populations.
+template <int PREC>
+__device__ __forceinline__ void place(const PhysGeom& G, int P, typename Store<PREC>::T* pop,
+                                      int x, int y, int z, const float (&g)[Q]) {
+  using S = Store<PREC>;
+  const size_t SS = G.slot_stride;
+  const size_t ln = lin(G, x, y, z);
+  S::st(pop, ln, g[0]);
+  static_for<0, 9>([&](auto PI) {
+    constexpr int pi = decltype(PI)::value;
+    constexpr int a = pair_a(pi), b = pair_b(pi);
+    auto* s0 = pop + (size_t)(1 + 2 * pi) * SS;
+    auto* s1 = s0 + SS;
+    S::st(P ? s0 : s1, lin_fwd<cx(a), cy(a), cz(a)>(G, x, y, z), g[a]);
+    S::st(P ? s1 : s0, ln, g[b]);
+  });
+}
+
+template <int PREC>
+__device__ __forceinline__ void fetch(const PhysGeom& G, int P, const typename Store<PREC>::T* pop,
+                                      int x, int y, int z, float (&g)[Q]) {
+  using S = Store<PREC>;
+  const size_t SS = G.slot_stride;
+  const size_t ln = lin(G, x, y, z);
+  g[0] = S::ld(pop, ln);
+  static_for<0, 9>([&](auto PI) {
+    constexpr int pi = decltype(PI)::value;
+    constexpr int a = pair_a(pi), b = pair_b(pi);
+    const auto* s0 = pop + (size_t)(1 + 2 * pi) * SS;
+    const auto* s1 = s0 + SS;
+    g[a] = S::ld(P ? s0 : s1, lin_fwd<cx(a), cy(a), cz(a)>(G, x, y, z));
+    g[b] = S::ld(P ? s1 : s0, ln);
+  });
+}
+
+// f = feq(rho, u) at every fluid node, stored for a parity-0 launch.
+template <int PREC>
+__global__ void __launch_bounds__(256)
+    k_phys_init(PhysGeom G, const float* __restrict__ rho_in, const float* __restrict__ u_in,
+                float rho0, float u0x, float u0y, float u0z, void* __restrict__ pop_v,
+                const uint8_t* __restrict__ flags, float* __restrict__ rho_o,
+                float* __restrict__ u_o) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z * blockDim.z + threadIdx.z;
+  if (x >= G.nx || y >= G.ny || z >= G.nz) return;
+  const size_t N = G.n;
+  const size_t nid = (size_t)x + (size_t)G.nx * ((size_t)y + (size_t)G.ny * (size_t)z);
+  if (flags[nid] & FLAG_SOLID) {
+    rho_o[nid] = 0.0f;
+    u_o[nid] = u_o[N + nid] = u_o[2 * N + nid] = 0.0f;
+    return;
+  }
+  float r = rho0, vx = u0x, vy = u0y, vz = u0z;
+  if (rho_in) r = rho_in[nid];
+  if (u_in) {
+    vx = u_in[nid];
+    vy = u_in[N + nid];
+    vz = u_in[2 * N + nid];
+  }
+  const float drho = r - 1.0f;
+  const float uu15 = 1.5f * (vx * vx + vy * vy + vz * vz);
+  float g[Q];
+  static_for<0, Q>([&](auto I) {
+    constexpr int i = decltype(I)::value;
+    const float cu = cx(i) * vx + cy(i) * vy + cz(i) * vz;
+    g[i] = wf(i) * (drho + r * (3.0f * cu + 4.5f * cu * cu - uu15));
+  });
+  place<PREC>(G, 0, reinterpret_cast<typename Store<PREC>::T*>(pop_v), x, y, z, g);
+  rho_o[nid] = r;
+  u_o[nid] = vx;
+  u_o[N + nid] = vy;
+  u_o[2 * N + nid] = vz;
+}
+
+template <int PREC>
+__global__ void __launch_bounds__(256)
+    k_phys_read(PhysGeom G, int P, const void* __restrict__ pop_v, const uint8_t* __restrict__ flags,
+                float* __restrict__ out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z * blockDim.z + threadIdx.z;
+  if (x >= G.nx || y >= G.ny || z >= G.nz) return;
+  const size_t nid = (size_t)x + (size_t)G.nx * ((size_t)y + (size_t)G.ny * (size_t)z);
+  float g[Q];
+  if (flags[nid] & FLAG_SOLID) {
+    static_for<0, Q>([&](auto I) { out[(size_t)I.value * G.n + nid] = 0.0f; });
+    return;
+  }
+  fetch<PREC>(G, P, reinterpret_cast<const typename Store<PREC>::T*>(pop_v), x, y, z, g);
+  static_for<0, Q>([&](auto I) {
+    constexpr int i = decltype(I)::value;
+    out[(size_t)i * G.n + nid] = g[i] + wf(i);
+  });
+}
+
+template <int PREC>
+__global__ void __launch_bounds__(256)
+    k_phys_write(PhysGeom G, int P, void* __restrict__ pop_v, const uint8_t* __restrict__ flags,
+                 const float* __restrict__ in) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z * blockDim.z + threadIdx.z;
+  if (x >= G.nx || y >= G.ny || z >= G.nz) return;
+  const size_t nid = (size_t)x + (size_t)G.nx * ((size_t)y + (size_t)G.ny * (size_t)z);
+  if (flags[nid] & FLAG_SOLID) return;
+  float g[Q];
+  static_for<0, Q>([&](auto I) {
+    constexpr int i = decltype(I)::value;
+    g[i] = in[(size_t)i * G.n + nid] - wf(i);
+  });
+  place<PREC>(G, P, reinterpret_cast<typename Store<PREC>::T*>(pop_v), x, y, z, g);
+}
+
+dim3 phys_block() { return dim3(32, 4, 2); }
+dim3 phys_grid(const PhysGeom& g) {
+  const dim3 b = phys_block();
+  return dim3((g.nx + b.x - 1) / b.x, (g.ny + b.y - 1) / b.y, (g.nz + b.z - 1) / b.z);
+}
+
+template <int PREC, int COLL, bool SMAG, bool FORCE>
+cudaError_t launch_step(const Ctx& c, int P, bool wm, cudaStream_t s) {
+  const PhysGeom& G = c.pp.g;
+  if (wm)
+    k_phys_step<PREC, COLL, SMAG, FORCE, true><<<phys_grid(G), phys_block(), 0, s>>>(
+        c.pp, P, c.pop, c.flags, c.links, c.rho, c.u, c.status);
+  else
+    k_phys_step<PREC, COLL, SMAG, FORCE, false><<<phys_grid(G), phys_block(), 0, s>>>(
+        c.pp, P, c.pop, c.flags, c.links, c.rho, c.u, c.status);
+  return cudaGetLastError();
+}
+
+template <int PREC, int COLL, bool SMAG>
+cudaError_t dispatch_force(const Ctx& c, int P, bool wm, cudaStream_t s) {
+  const bool force = c.pp.accel[0] != 0.f || c.pp.accel[1] != 0.f || c.pp.accel[2] != 0.f;
+  return force ? launch_step<PREC, COLL, SMAG, true>(c, P, wm, s)
+               : launch_step<PREC, COLL, SMAG, false>(c, P, wm, s);
+}
+
+template <int PREC, int COLL>
+cudaError_t dispatch_smag(const Ctx& c, int P, bool wm, cudaStream_t s) {
+  return c.pp.smag_cs > 0.f ? dispatch_force<PREC, COLL, true>(c, P, wm, s)
+                            : dispatch_force<PREC, COLL, false>(c, P, wm, s);
+}
+
+template <int PREC>
+cudaError_t dispatch_coll(const Ctx& c, int P, bool wm, cudaStream_t s) {
+  return c.d.collision == LBM_COLL_TRT ? dispatch_smag<PREC, LBM_COLL_TRT>(c, P, wm, s)
+                                       : dispatch_smag<PREC, LBM_COLL_BGK>(c, P, wm, s);
+}
+
+}  // namespace
+
+cudaError_t phys_step(const Ctx& c, int parity, bool write_moments, cudaStream_t s) {
+  switch (c.d.precision) {
+    case LBM_PREC_F32: return dispatch_coll<LBM_PREC_F32>(c, parity, write_moments, s);
+    case LBM_PREC_F16S: return dispatch_coll<LBM_PREC_F16S>(c, parity, write_moments, s);
+    default: return dispatch_coll<LBM_PREC_BF16S>(c, parity, write_moments, s);
+  }
+}
+
+cudaError_t phys_init(const Ctx& c, const float* rho, const float* u3, float rho0, const float* u0,
+                      cudaStream_t s) {
+  const float zero[3] = {0.f, 0.f, 0.f};
+  if (!u0) u0 = zero;
+  const PhysGeom& G = c.pp.g;
+  switch (c.d.precision) {
+    case LBM_PREC_F32:
+      k_phys_init<LBM_PREC_F32><<<phys_grid(G), phys_block(), 0, s>>>(
+          G, rho, u3, rho0, u0[0], u0[1], u0[2], c.pop, c.flags, c.rho, c.u);
+      break;
+    case LBM_PREC_F16S:
+      k_phys_init<LBM_PREC_F16S><<<phys_grid(G), phys_block(), 0, s>>>(
+          G, rho, u3, rho0, u0[0], u0[1], u0[2], c.pop, c.flags, c.rho, c.u);
+      break;
+    default:
+      k_phys_init<LBM_PREC_BF16S><<<phys_grid(G), phys_block(), 0, s>>>(
+          G, rho, u3, rho0, u0[0], u0[1], u0[2], c.pop, c.flags, c.rho, c.u);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t phys_read_pops(const Ctx& c, float* out, cudaStream_t s) {
+  const PhysGeom& G = c.pp.g;
+  switch (c.d.precision) {
+    case LBM_PREC_F32:
+      k_phys_read<LBM_PREC_F32><<<phys_grid(G), phys_block(), 0, s>>>(G, c.parity, c.pop, c.flags, out);
+      break;
+    case LBM_PREC_F16S:
+      k_phys_read<LBM_PREC_F16S><<<phys_grid(G), phys_block(), 0, s>>>(G, c.parity, c.pop, c.flags, out);
+      break;
+    default:
+      k_phys_read<LBM_PREC_BF16S><<<phys_grid(G), phys_block(), 0, s>>>(G, c.parity, c.pop, c.flags, out);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t phys_write_pops(const Ctx& c, const float* in, cudaStream_t s) {
+  const PhysGeom& G = c.pp.g;
+  switch (c.d.precision) {
+    case LBM_PREC_F32:
+      k_phys_write<LBM_PREC_F32><<<phys_grid(G), phys_block(), 0, s>>>(G, c.parity, c.pop, c.flags, in);
+      break;
+    case LBM_PREC_F16S:
+      k_phys_write<LBM_PREC_F16S><<<phys_grid(G), phys_block(), 0, s>>>(G, c.parity, c.pop, c.flags, in);
+      break;
+    default:
+      k_phys_write<LBM_PREC_BF16S><<<phys_grid(G), phys_block(), 0, s>>>(G, c.parity, c.pop, c.flags, in);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace lbm

@@ -1,0 +1,327 @@
+"""Python host layer over the C ABI of liblbm_b200.so (include/lbm.h).
+
+It mirrors the reference sim host (volumetric-grid/lattice-boltzmann/src/
+main.cpp): the tier and preset tables (:103-135), apply_preset (:1167-1211),
+the substep chain (:1554-1591) and the moment readback (:1288-1314).  All
+compute goes through the CUDA library; there is no CPU fallback: if the
+library is missing, importing a Lattice raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = Path(os.environ.get("LBM_B200_LIB", _HERE / "liblbm_b200.so"))
+
+# status codes (include/lbm.h)
+OK = 0
+ERR_INVALID_ARG = -1
+ERR_CUDA = -2
+ERR_NO_DEVICE = -3
+ERR_OUT_OF_MEMORY = -4
+ERR_STATE = -5
+ERR_UNSUPPORTED = -6
+ERR_TIMEOUT = -7
+ERR_NONFINITE = -8
+ERR_IO = -9
+
+MODE_REFERENCE, MODE_PHYSICS = 0, 1
+PREC_F32, PREC_F16S, PREC_BF16S = 0, 1, 2
+COLL_BGK, COLL_TRT = 0, 1
+UROUND_NONE, UROUND_RTE, UROUND_RTZ = 0, 1, 2
+U_F32X3, U_F16X4, U_F32X4 = 0, 1, 2
+FACE_XM, FACE_XP, FACE_YM, FACE_YP, FACE_ZM, FACE_ZP = range(6)
+
+ERR_NAMES = {OK: "OK", ERR_INVALID_ARG: "INVALID_ARG", ERR_CUDA: "CUDA", ERR_NO_DEVICE: "NO_DEVICE",
+             ERR_OUT_OF_MEMORY: "OUT_OF_MEMORY", ERR_STATE: "STATE", ERR_UNSUPPORTED: "UNSUPPORTED",
+             ERR_TIMEOUT: "TIMEOUT", ERR_NONFINITE: "NONFINITE", ERR_IO: "IO"}
+
+
+class LbmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Desc(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_uint32),
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+        ("mode", C.c_int32), ("precision", C.c_int32), ("collision", C.c_int32),
+        ("periodic", C.c_int32 * 3),
+        ("tau", C.c_float), ("trt_magic", C.c_float), ("smagorinsky_cs", C.c_float),
+        ("body_accel", C.c_float * 3),
+        ("wall_velocity", (C.c_float * 3) * 6),
+        ("u_inf", C.c_float * 3), ("rho0", C.c_float),
+        ("ref_inlet_outlet", C.c_int32), ("ref_free_slip", C.c_int32), ("ref_u_round", C.c_int32),
+    ]
+
+
+class Info(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_uint32),
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+        ("mode", C.c_int32), ("precision", C.c_int32),
+        ("iteration", C.c_uint64), ("device_bytes", C.c_uint64),
+        ("bytes_per_node", C.c_double), ("layout", C.c_int32), ("device", C.c_int32),
+    ]
+
+
+# Every symbol include/lbm.h declares, with its ctypes signature.
+_P = C.c_void_p
+_SIGS = {
+    "lbm_desc_default": (C.c_int, [C.POINTER(Desc)]),
+    "lbm_create": (C.c_int, [C.POINTER(Desc), C.POINTER(_P)]),
+    "lbm_destroy": (C.c_int, [_P]),
+    "lbm_set_stream": (C.c_int, [_P, _P]),
+    "lbm_set_flags": (C.c_int, [_P, _P, C.c_size_t]),
+    "lbm_read_classification": (C.c_int, [_P, _P, C.c_size_t]),
+    "lbm_init_equilibrium": (C.c_int, [_P, C.c_float, C.POINTER(C.c_float)]),
+    "lbm_init_from_moments": (C.c_int, [_P, _P, _P, C.c_int]),
+    "lbm_step": (C.c_int, [_P, C.c_int]),
+    "lbm_sync": (C.c_int, [_P]),
+    "lbm_read_moments": (C.c_int, [_P, _P, _P, C.c_int]),
+    "lbm_device_moments": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P)]),
+    "lbm_conservation": (C.c_int, [_P, C.POINTER(C.c_double)]),
+    "lbm_read_populations": (C.c_int, [_P, _P, C.c_size_t]),
+    "lbm_write_populations": (C.c_int, [_P, _P, C.c_size_t]),
+    "lbm_get_info": (C.c_int, [_P, C.POINTER(Info)]),
+    "lbm_last_error": (C.c_char_p, [_P]),
+    "lbm_lattice_tables": (C.c_int, [_P, _P, _P]),
+    "lbm_voxelize_naca": (C.c_int, [C.c_char_p, C.c_int32, C.c_int32, C.c_int32, C.c_float,
+                                    C.c_float, C.c_float, _P, C.c_size_t]),
+    "lbm_half_to_float": (C.c_int, [_P, _P, C.c_size_t]),
+    "lbm_build_info": (C.c_char_p, []),
+}
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Loads the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise LbmError(ERR_STATE, f"{LIB_PATH} is missing: build it with gpu-sims_b200/build.py")
+        lib = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def _check(rc: int, ctx=None) -> None:
+    if rc != OK:
+        msg = load().lbm_last_error(ctx).decode()
+        raise LbmError(rc, msg)
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def build_info() -> str:
+    return load().lbm_build_info().decode()
+
+
+def lattice_tables():
+    """(c[19,3] int32, w[19] float32, opp[19] int32) in the reference order."""
+    c = np.zeros((19, 3), np.int32)
+    w = np.zeros(19, np.float32)
+    o = np.zeros(19, np.int32)
+    _check(load().lbm_lattice_tables(_ptr(c), _ptr(w), _ptr(o)))
+    return c, w, o
+
+
+def voxelize_naca(designation: str, nx: int, ny: int, nz: int, chord_frac: float = 0.25,
+                  center_x_frac: float = 0.25, angle_of_attack_deg: float = 0.0) -> np.ndarray:
+    """Obstacle mask (uint8, x-fastest flat array) of a NACA 4-digit airfoil."""
+    m = np.zeros(nx * ny * nz, np.uint8)
+    _check(load().lbm_voxelize_naca(designation.encode(), nx, ny, nz, chord_frac, center_x_frac,
+                                    angle_of_attack_deg, _ptr(m), m.size))
+    return m
+
+
+def half_to_float(h: np.ndarray) -> np.ndarray:
+    h = np.ascontiguousarray(h, dtype=np.uint16)
+    out = np.empty(h.shape, np.float32)
+    _check(load().lbm_half_to_float(_ptr(h), _ptr(out), h.size))
+    return out
+
+
+def default_desc(**kw) -> Desc:
+    d = Desc()
+    _check(load().lbm_desc_default(C.byref(d)))
+    for k, v in kw.items():
+        if k in ("periodic", "body_accel", "u_inf"):
+            arr = getattr(d, k)
+            for i, x in enumerate(v):
+                arr[i] = x
+        elif k == "wall_velocity":
+            for f, vec in enumerate(v):
+                for a, x in enumerate(vec):
+                    d.wall_velocity[f][a] = x
+        else:
+            setattr(d, k, v)
+    return d
+
+
+class Lattice:
+    """One D3Q19 domain on the current CUDA device (wraps an lbm_ctx)."""
+
+    def __init__(self, desc: Desc | None = None, **kw):
+        lib = load()
+        self.desc = desc if desc is not None else default_desc(**kw)
+        h = _P()
+        _check(lib.lbm_create(C.byref(self.desc), C.byref(h)))
+        self._h = h
+        self.shape = (self.desc.nx, self.desc.ny, self.desc.nz)
+        self.n = self.desc.nx * self.desc.ny * self.desc.nz
+
+    # context lifetime -------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            load().lbm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _c(self, rc: int) -> None:
+        _check(rc, self._h)
+
+    # API ---------------------------------------------------------------------
+    def set_stream(self, stream_ptr: int | None) -> None:
+        self._c(load().lbm_set_stream(self._h, stream_ptr))
+
+    def set_flags(self, mask: np.ndarray) -> None:
+        m = np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
+        self._c(load().lbm_set_flags(self._h, _ptr(m), m.size))
+
+    def read_classification(self) -> np.ndarray:
+        out = np.zeros(self.n, np.uint32)
+        self._c(load().lbm_read_classification(self._h, _ptr(out), out.size))
+        return out
+
+    def init_equilibrium(self, rho0: float = 1.0, u0=(0.0, 0.0, 0.0)) -> None:
+        u = (C.c_float * 3)(*u0)
+        self._c(load().lbm_init_equilibrium(self._h, rho0, u))
+
+    def init_from_moments(self, rho: np.ndarray, u: np.ndarray, fmt: int = U_F32X3) -> None:
+        r = np.ascontiguousarray(rho, dtype=np.float32).reshape(-1)
+        dt = np.uint16 if fmt == U_F16X4 else np.float32
+        uu = np.ascontiguousarray(u, dtype=dt)
+        self._c(load().lbm_init_from_moments(self._h, _ptr(r), _ptr(uu), fmt))
+
+    def step(self, nsteps: int = 1) -> None:
+        self._c(load().lbm_step(self._h, nsteps))
+
+    def sync(self) -> None:
+        self._c(load().lbm_sync(self._h))
+
+    def read_moments(self, fmt: int = U_F32X3):
+        rho = np.empty(self.n, np.float32)
+        if fmt == U_F32X3:
+            u = np.empty((self.n, 3), np.float32)
+        elif fmt == U_F32X4:
+            u = np.empty((self.n, 4), np.float32)
+        else:
+            u = np.empty((self.n, 4), np.uint16)
+        self._c(load().lbm_read_moments(self._h, _ptr(rho), _ptr(u), fmt))
+        return rho, u
+
+    def device_moments(self):
+        r, u = _P(), _P()
+        self._c(load().lbm_device_moments(self._h, C.byref(r), C.byref(u)))
+        return r.value, u.value
+
+    def conservation(self) -> np.ndarray:
+        out = (C.c_double * 4)()
+        self._c(load().lbm_conservation(self._h, out))
+        return np.array(out[:], np.float64)
+
+    def read_populations(self) -> np.ndarray:
+        f = np.empty((19, self.n), np.float32)
+        self._c(load().lbm_read_populations(self._h, _ptr(f), f.size))
+        return f
+
+    def write_populations(self, f: np.ndarray) -> None:
+        ff = np.ascontiguousarray(f, dtype=np.float32)
+        self._c(load().lbm_write_populations(self._h, _ptr(ff), ff.size))
+
+    def info(self) -> Info:
+        i = Info()
+        i.struct_size = C.sizeof(Info)
+        self._c(load().lbm_get_info(self._h, C.byref(i)))
+        return i
+
+
+# --- mirror of the reference sim host ---------------------------------------
+
+@dataclass(frozen=True)
+class Tier:
+    label: str
+    nx: int
+    ny: int
+    nz: int
+
+
+@dataclass(frozen=True)
+class Preset:
+    label: str
+    naca: str
+    angle_of_attack_deg: float
+    u_inf: float
+    tau: float
+
+
+# TIERS and PRESETS of the reference (src/main.cpp:103-116, :122-135).
+TIERS = (Tier("128^3 (Laptop)", 128, 128, 128),
+         Tier("256x128x128 (Desktop)", 256, 128, 128),
+         Tier("512x256x256 (Capture)", 512, 256, 256))
+PRESETS = (Preset("NACA0012 - Low-Re", "0012", 4.0, 0.04, 0.60),
+           Preset("NACA0012 - Med-Re", "0012", 8.0, 0.06, 0.55),
+           Preset("NACA4412 - Med-Re", "4412", 6.0, 0.06, 0.55))
+AIRFOIL_CHORD_CENTER_X_FRAC = 0.25
+AIRFOIL_CHORD_LENGTH_FRAC = 0.25
+
+
+def preset_u_inf(p: Preset):
+    """update_u_inf_vector (src/main.cpp:1155-1160): |u| and AoA -> u_inf."""
+    a = np.float32(p.angle_of_attack_deg) * np.float32(0.01745329251994329576923690768489)
+    return (float(np.float32(p.u_inf) * np.float32(math.cos(a))),
+            float(np.float32(p.u_inf) * np.float32(math.sin(a))), 0.0)
+
+
+def preset_desc(preset_idx: int, nx: int, ny: int, nz: int) -> Desc:
+    p = PRESETS[preset_idx]
+    return default_desc(nx=nx, ny=ny, nz=nz, tau=p.tau, u_inf=preset_u_inf(p))
+
+
+def apply_preset(lat: Lattice, preset_idx: int) -> np.ndarray:
+    """apply_preset (src/main.cpp:1167-1211): voxelise the airfoil, upload the
+    mask, run the equilibrium init.  Returns the mask."""
+    p = PRESETS[preset_idx]
+    nx, ny, nz = lat.shape
+    mask = voxelize_naca(p.naca, nx, ny, nz, AIRFOIL_CHORD_LENGTH_FRAC, AIRFOIL_CHORD_CENTER_X_FRAC,
+                         p.angle_of_attack_deg)
+    lat.set_flags(mask)
+    lat.init_equilibrium(1.0, tuple(lat.desc.u_inf))
+    return mask

@@ -1,0 +1,212 @@
+/*
+ * lbm.h -- C ABI of the B200 D3Q19 lattice-Boltzmann step.
+ *
+ * This is the drop-in boundary for the `volumetric-grid/lattice-boltzmann`
+ * sim of GPU-Sims.  The reference has no plugin or FFI API: its step is wired
+ * directly into `main()` through Vulkan compute pipelines.  Each entry point
+ * below names the reference code it replaces (paths relative to
+ * `volumetric-grid/lattice-boltzmann/` unless stated otherwise).
+ *
+ * Conventions
+ *  - Every call returns an int status: LBM_OK (0) or a negative LBM_ERR_*.
+ *    No C++ exception crosses the ABI.  lbm_last_error() gives the message.
+ *  - A context owns all of its device memory.  Host pointers passed in are
+ *    borrowed for the duration of the call only.
+ *  - Grids are linearised x-fastest: index = x + Nx*(y + Ny*z), exactly as
+ *    the reference's obstacle mask (src/main.cpp:307) and capture buffers.
+ *  - One context is driven by one host thread at a time, on one CUDA stream
+ *    (lbm_set_stream; default: a stream the context creates).
+ *  - Work is enqueued asynchronously on that stream; calls that return host
+ *    data (read_*, conservation, sync) synchronise the stream first.
+ */
+#ifndef LBM_B200_H
+#define LBM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define LBM_API __attribute__((visibility("default")))
+#else
+#define LBM_API
+#endif
+
+#define LBM_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+#define LBM_OK                 0
+#define LBM_ERR_INVALID_ARG   -1  /* bad pointer, size, enum or range        */
+#define LBM_ERR_CUDA          -2  /* a CUDA runtime call failed               */
+#define LBM_ERR_NO_DEVICE     -3  /* no CUDA device visible to this process   */
+#define LBM_ERR_OUT_OF_MEMORY -4  /* device allocation failed                 */
+#define LBM_ERR_STATE         -5  /* call out of order (e.g. step before init)*/
+#define LBM_ERR_UNSUPPORTED   -6  /* option combination not built             */
+#define LBM_ERR_TIMEOUT       -7  /* a bounded device-side wait gave up       */
+#define LBM_ERR_NONFINITE     -8  /* NaN/Inf or rho<=0 found at a fluid node  */
+#define LBM_ERR_IO            -9  /* capture file could not be read/written   */
+
+/* ---- enums ------------------------------------------------------------- */
+/* Semantics of the step.
+ *  REFERENCE: the reference's four-pass step, reproduced literally:
+ *    collide (shaders/collide.comp.glsl:39-61) with the lagged moments and
+ *    velocity rounded to fp16 (the rgba16f image, src/main.cpp:843);
+ *    clamp-to-edge pull stream (shaders/stream.comp.glsl:29-47);
+ *    apply_boundaries (shaders/apply_boundaries.comp.glsl:57-169): solid
+ *    zeroing, post-stream bounce-back against the mask with out-of-bounds
+ *    counted as solid, equilibrium inlet/outlet, inverted free-slip;
+ *    compute_moments (shaders/compute_moments.comp.glsl:29-50).
+ *  PHYSICS: textbook stream-collide: periodic or half-way bounce-back faces,
+ *    momentum-corrected moving walls, BGK or TRT, optional Smagorinsky and
+ *    Guo body force.  Not present in the reference. */
+enum lbm_mode      { LBM_MODE_REFERENCE = 0, LBM_MODE_PHYSICS = 1 };
+/* Population storage.  F16S/BF16S store f_i - w_i (physics mode only);
+ * collision arithmetic is fp32 in every case. */
+enum lbm_precision { LBM_PREC_F32 = 0, LBM_PREC_F16S = 1, LBM_PREC_BF16S = 2 };
+enum lbm_collision { LBM_COLL_BGK = 0, LBM_COLL_TRT = 1 };
+/* Rounding applied to u between moments and the next collide (reference
+ * mode).  Vulkan allows RTE or RTZ for float->half image stores. */
+enum lbm_u_round   { LBM_UROUND_NONE = 0, LBM_UROUND_RTE = 1, LBM_UROUND_RTZ = 2 };
+/* Host velocity formats for init/readback. */
+enum lbm_u_format  { LBM_U_F32X3 = 0,   /* float[N][3]                        */
+                     LBM_U_F16X4 = 1,   /* uint16 half[N][4], w=0: rgba16f    */
+                     LBM_U_F32X4 = 2 }; /* float[N][4], w=0                   */
+/* Faces, for per-face wall velocities: x-, x+, y-, y+, z-, z+. */
+enum lbm_face { LBM_FACE_XM = 0, LBM_FACE_XP, LBM_FACE_YM, LBM_FACE_YP,
+                LBM_FACE_ZM, LBM_FACE_ZP };
+
+/* ---- descriptor -------------------------------------------------------- */
+typedef struct lbm_desc {
+    uint32_t struct_size;       /* sizeof(lbm_desc), for ABI growth          */
+    int32_t  nx, ny, nz;        /* lattice nodes; each >= 2                  */
+    int32_t  mode;              /* enum lbm_mode                             */
+    int32_t  precision;         /* enum lbm_precision                        */
+    int32_t  collision;         /* enum lbm_collision (physics mode)         */
+    int32_t  periodic[3];       /* physics mode: 1 = periodic axis, 0 = wall */
+    float    tau;               /* BGK relaxation time (> 0.5)               */
+    float    trt_magic;         /* TRT Lambda; default 3/16                  */
+    float    smagorinsky_cs;    /* 0 = off                                   */
+    float    body_accel[3];     /* Guo force density F = rho * body_accel    */
+    float    wall_velocity[6][3]; /* physics mode: moving-wall velocity per
+                                   face (enum lbm_face); 0 = resting wall    */
+    /* reference-mode knobs (src/main.cpp:1523-1537 uniforms) */
+    float    u_inf[3];          /* inlet / init velocity (BoundariesUniforms) */
+    float    rho0;              /* boundary density, RHO_0 = 1 (:90)          */
+    int32_t  ref_inlet_outlet;  /* regime 3 of apply_boundaries: 1 = on       */
+    int32_t  ref_free_slip;     /* regime 4 of apply_boundaries: 1 = on       */
+    int32_t  ref_u_round;       /* enum lbm_u_round, default RTE              */
+} lbm_desc;
+
+typedef struct lbm_info {
+    uint32_t struct_size;
+    int32_t  nx, ny, nz;
+    int32_t  mode, precision;
+    uint64_t iteration;          /* steps taken since the last init          */
+    uint64_t device_bytes;       /* device memory the context owns           */
+    double   bytes_per_node;     /* algorithmic HBM bytes of one node update */
+    int32_t  layout;             /* 0 = two-buffer pull, 1 = esoteric pull   */
+    int32_t  device;             /* CUDA ordinal                             */
+} lbm_info;
+
+typedef struct lbm_ctx lbm_ctx;
+
+/* Fills *d with the reference defaults: 64^3, reference mode, fp32, BGK,
+ * tau = TAU_DEFAULT 0.6 (src/main.cpp:84), rho0 = 1, all regimes on,
+ * u rounding RTE, TRT Lambda 3/16, no force, resting walls. */
+LBM_API int lbm_desc_default(lbm_desc* d);
+
+/* Allocates a context on the current CUDA device.
+ * Replaces allocate_tier_images (src/main.cpp:835-846) and the pipeline
+ * creation that follows it.  The lattice starts all-fluid. */
+LBM_API int lbm_create(const lbm_desc* desc, lbm_ctx** out);
+LBM_API int lbm_destroy(lbm_ctx* ctx);
+
+/* Uses `stream` (a cudaStream_t) for all later work; NULL = the context's
+ * own stream. */
+LBM_API int lbm_set_stream(lbm_ctx* ctx, void* stream);
+
+/* Uploads the obstacle mask (uint8, Nx*Ny*Nz bytes, x-fastest; value 1 =
+ * solid, any other value = fluid, as `mask_at(c) == 1u` in
+ * shaders/apply_boundaries.comp.glsl:52-55,62) and classifies every node.
+ * Replaces obstacle_mask.upload (src/main.cpp:1190, :1366). */
+LBM_API int lbm_set_flags(lbm_ctx* ctx, const uint8_t* mask, size_t n);
+
+/* Reads the per-node classification word: bit 0 = node is solid; bit i
+ * (1..18) = mask at x + c_i is solid, out-of-bounds counting as solid on
+ * non-periodic axes (shaders/apply_boundaries.comp.glsl:52-55,76-79). */
+LBM_API int lbm_read_classification(lbm_ctx* ctx, uint32_t* out, size_t n);
+
+/* Equilibrium initialisation.  Replaces the init_equilibrium dispatch
+ * (shaders/init_equilibrium.comp.glsl:35-47; src/main.cpp:1193-1206):
+ * f_i = feq_i(rho0, u0) at every node, moments = (rho0, u0). */
+LBM_API int lbm_init_equilibrium(lbm_ctx* ctx, float rho0, const float u0[3]);
+
+/* Initialises f = feq(rho(x), u(x)) from host moment fields.  This is the
+ * capture resume that the reference's F9 path intends (src/main.cpp:1359-
+ * 1383) but does not do: its init shader ignores the uploaded moments.
+ * u_fmt: LBM_U_F32X3, LBM_U_F32X4 or LBM_U_F16X4 (capture `velocity`). */
+LBM_API int lbm_init_from_moments(lbm_ctx* ctx, const float* rho, const void* u,
+                          int u_fmt);
+
+/* Advances nsteps steps.  Replaces the substep dispatch chain
+ * collide -> stream -> boundaries -> moments (src/main.cpp:1554-1591).
+ * The moments of the last step are written for readback. */
+LBM_API int lbm_step(lbm_ctx* ctx, int nsteps);
+
+/* Waits for the context's stream; returns LBM_ERR_NONFINITE if a NaN/Inf or
+ * non-positive density was seen at a fluid node since the last sync. */
+LBM_API int lbm_sync(lbm_ctx* ctx);
+
+/* Copies rho (float[N]) and u (format u_fmt) to host memory; either pointer
+ * may be NULL.  Solid nodes read rho = 0, u = 0
+ * (shaders/compute_moments.comp.glsl:45-47).  Replaces the rho/velocity
+ * Image::readback in capture_save and the VDB export (src/main.cpp:1290-
+ * 1296, :1771-1779). */
+LBM_API int lbm_read_moments(lbm_ctx* ctx, float* rho, void* u, int u_fmt);
+
+/* Device pointers of the moment fields (rho float[N]; u float[3][N],
+ * planes x, y, z) for on-device consumers.  Headless replacement of the
+ * `velocity_image` texture bindings (src/main.cpp:1106-1114). */
+LBM_API int lbm_device_moments(lbm_ctx* ctx, const float** d_rho, const float** d_u);
+
+/* out[0] = sum rho, out[1..3] = sum rho*u over fluid nodes, in fp64. */
+LBM_API int lbm_conservation(lbm_ctx* ctx, double out[4]);
+
+/* Full population state, natural layout float[19][N] (direction-major),
+ * post-collision populations of the current step.  For checkpoints. */
+LBM_API int lbm_read_populations(lbm_ctx* ctx, float* f, size_t n);
+LBM_API int lbm_write_populations(lbm_ctx* ctx, const float* f, size_t n);
+
+LBM_API int lbm_get_info(lbm_ctx* ctx, lbm_info* info);
+
+/* Message of the last failed call on ctx (or on this thread if ctx is
+ * NULL).  Never NULL. */
+LBM_API const char* lbm_last_error(lbm_ctx* ctx);
+
+/* ---- host-side helpers (no GPU needed) --------------------------------- */
+
+/* D3Q19 tables in the reference's direction order
+ * (shaders/lattice_constants.glsl:23-75): c[19][3], w[19], opp[19]. */
+LBM_API int lbm_lattice_tables(int32_t* c, float* w, int32_t* opp);
+
+/* NACA 4-digit airfoil voxeliser, extruded in z.  Restates
+ * naca::voxelize_into (src/main.cpp:254-312) with the preset geometry of
+ * apply_preset (src/main.cpp:1180-1190): chord = chord_frac*Nx, leading edge
+ * at (center_x_frac*Nx - chord/2, Ny/2). */
+LBM_API int lbm_voxelize_naca(const char* designation, int32_t nx, int32_t ny,
+                      int32_t nz, float chord_frac, float center_x_frac,
+                      float angle_of_attack_deg, uint8_t* mask, size_t n);
+
+/* binary16 -> binary32, as half_to_float (src/main.cpp:320-337). */
+LBM_API int lbm_half_to_float(const uint16_t* h, float* f, size_t n);
+
+/* Library build string (compiler, arch, ABI version). */
+LBM_API const char* lbm_build_info(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LBM_B200_H */

@@ -1,0 +1,174 @@
+"""ctypes front end of the CPU oracle (liboracle.so, built from lbm_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and the CPU
+baseline legs of bench.py use this module, and only as the checker or the
+timed CPU baseline; the product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+
+_lib = None
+_P = C.c_void_p
+
+
+def build() -> Path:
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        L = C.CDLL(str(LIB))
+        sigs = {
+            "oracle_set_threads": (None, [C.c_int]),
+            "oracle_max_threads": (C.c_int, []),
+            "oracle_tables": (None, [_P, _P, _P]),
+            "oracle_feq_f64": (None, [C.c_double] * 4 + [_P]),
+            "oracle_feq_f32": (None, [C.c_float] * 4 + [_P]),
+            "oracle_round_f16": (C.c_float, [C.c_float, C.c_int]),
+            "oracle_classify": (None, [C.c_int, C.c_int, C.c_int, _P, _P, _P]),
+            "oracle_ref_init": (None, [_P, _P, _P, _P, C.c_float, _P, _P, _P, _P]),
+            "oracle_ref_step": (None, [_P, _P, _P, _P, _P, _P, C.c_int]),
+            "oracle_ref_collided": (None, [_P, _P, _P, _P, _P, _P]),
+            "oracle_ext_init_f64": (None, [_P] * 6),
+            "oracle_ext_init_f32": (None, [_P] * 6),
+            "oracle_ext_step_f64": (None, [_P, _P, _P, _P, C.c_int, _P, _P]),
+            "oracle_ext_step_f32": (None, [_P, _P, _P, _P, C.c_int, _P, _P]),
+            "oracle_voxelize_naca": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_float,
+                                               C.c_float, C.c_float, _P]),
+        }
+        for name, (res, args) in sigs.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _p(a) -> int | None:
+    return None if a is None else a.ctypes.data
+
+
+def set_threads(n: int) -> None:
+    lib().oracle_set_threads(n)
+
+
+def max_threads() -> int:
+    return lib().oracle_max_threads()
+
+
+def tables():
+    c = np.zeros((19, 3), np.int32)
+    w = np.zeros(19, np.float64)
+    o = np.zeros(19, np.int32)
+    lib().oracle_tables(_p(c), _p(w), _p(o))
+    return c, w, o
+
+
+def feq_f64(rho, ux, uy, uz) -> np.ndarray:
+    out = np.zeros(19, np.float64)
+    lib().oracle_feq_f64(rho, ux, uy, uz, _p(out))
+    return out
+
+
+def feq_f32(rho, ux, uy, uz) -> np.ndarray:
+    out = np.zeros(19, np.float32)
+    lib().oracle_feq_f32(rho, ux, uy, uz, _p(out))
+    return out
+
+
+def round_f16(v: float, mode: int = 1) -> float:
+    return lib().oracle_round_f16(v, mode)
+
+
+def classify(mask: np.ndarray, shape, periodic=(0, 0, 0)) -> np.ndarray:
+    nx, ny, nz = shape
+    m = np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
+    per = np.array(periodic, np.int32)
+    out = np.zeros(nx * ny * nz, np.uint32)
+    lib().oracle_classify(nx, ny, nz, _p(per), _p(m), _p(out))
+    return out
+
+
+def voxelize_naca(designation, nx, ny, nz, chord_frac=0.25, center_x_frac=0.25, aoa_deg=0.0):
+    m = np.zeros(nx * ny * nz, np.uint8)
+    lib().oracle_voxelize_naca(designation.encode(), nx, ny, nz, chord_frac, center_x_frac, aoa_deg, _p(m))
+    return m
+
+
+class RefState:
+    """The reference's state between substeps: ping populations float[19][N]
+    and the rho / u moment images (u kept unrounded; the collide rounds)."""
+
+    def __init__(self, shape, tau=0.6, u_inf=(0.0, 0.0, 0.0), rho0=1.0, inlet_outlet=1,
+                 free_slip=1, u_round=1, mask=None):
+        self.shape = tuple(shape)
+        nx, ny, nz = self.shape
+        self.n = nx * ny * nz
+        self.ip = np.array([nx, ny, nz, inlet_outlet, free_slip, u_round], np.int32)
+        self.fp = np.array([tau, u_inf[0], u_inf[1], u_inf[2], rho0], np.float32)
+        self.mask = np.zeros(self.n, np.uint8) if mask is None else np.ascontiguousarray(mask, np.uint8).reshape(-1)
+        self.f = np.zeros((19, self.n), np.float32)
+        self.rho = np.zeros(self.n, np.float32)
+        self.u = np.zeros((3, self.n), np.float32)
+
+    def init(self, rho0=1.0, u0=(0.0, 0.0, 0.0), rho=None, u=None):
+        """u: float[3][N] planes or None."""
+        u0a = np.array(u0, np.float32)
+        r = None if rho is None else np.ascontiguousarray(rho, np.float32).reshape(-1)
+        uu = None if u is None else np.ascontiguousarray(u, np.float32).reshape(3, -1)
+        lib().oracle_ref_init(_p(self.ip), _p(self.fp), _p(r), _p(uu), rho0, _p(u0a),
+                              _p(self.f), _p(self.rho), _p(self.u))
+
+    def step(self, n=1):
+        lib().oracle_ref_step(_p(self.ip), _p(self.fp), _p(self.mask), _p(self.f), _p(self.rho),
+                              _p(self.u), n)
+
+    def collided(self) -> np.ndarray:
+        """Post-collision populations of the next step (what the fused GPU
+        kernel keeps between launches)."""
+        out = np.zeros_like(self.f)
+        lib().oracle_ref_collided(_p(self.ip), _p(self.fp), _p(self.f), _p(self.rho), _p(self.u), _p(out))
+        return out
+
+
+class ExtState:
+    """Textbook stream-collide state: post-collision populations float[19][N]."""
+
+    def __init__(self, shape, periodic=(0, 0, 0), tau=0.6, collision=0, trt_magic=3.0 / 16.0,
+                 smag_cs=0.0, accel=(0.0, 0.0, 0.0), wall=None, mask=None, dtype=np.float64):
+        self.shape = tuple(shape)
+        nx, ny, nz = self.shape
+        self.n = nx * ny * nz
+        self.dtype = np.dtype(dtype)
+        self.ip = np.array([nx, ny, nz, *periodic, collision], np.int32)
+        w = np.zeros((6, 3)) if wall is None else np.asarray(wall, np.float64).reshape(6, 3)
+        self.dp = np.concatenate([[tau, trt_magic, smag_cs], np.asarray(accel, np.float64), w.reshape(-1)])
+        self.dp = np.ascontiguousarray(self.dp, np.float64)
+        self.mask = np.zeros(self.n, np.uint8) if mask is None else np.ascontiguousarray(mask, np.uint8).reshape(-1)
+        self.f = np.zeros((19, self.n), self.dtype)
+        self.rho = np.zeros(self.n, self.dtype)
+        self.u = np.zeros((3, self.n), self.dtype)
+
+    def init(self, rho, u):
+        r = np.ascontiguousarray(np.broadcast_to(rho, (self.n,)), self.dtype)
+        uu = np.ascontiguousarray(np.asarray(u, self.dtype).reshape(3, -1) * np.ones((3, self.n)), self.dtype)
+        fn = lib().oracle_ext_init_f64 if self.dtype == np.float64 else lib().oracle_ext_init_f32
+        fn(_p(self.ip), _p(self.dp), _p(self.mask), _p(r), _p(uu), _p(self.f))
+        self.rho[:] = np.where(self.mask == 1, 0, r)
+        self.u[:] = np.where(self.mask == 1, 0, uu)
+
+    def step(self, n=1):
+        fn = lib().oracle_ext_step_f64 if self.dtype == np.float64 else lib().oracle_ext_step_f32
+        fn(_p(self.ip), _p(self.dp), _p(self.mask), _p(self.f), n, _p(self.rho), _p(self.u))
