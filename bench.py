@@ -208,7 +208,11 @@ def run_ours(args, world, rank, local):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
-    stream = torch.cuda.current_stream()
+    # A dedicated stream: the library runs on it and the CUDA events are
+    # recorded on it.  (The legacy default stream has handle 0, which
+    # lbm_set_stream reads as "the context's own stream".)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
 
     def barrier():
         if world > 1:

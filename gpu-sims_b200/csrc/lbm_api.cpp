@@ -207,7 +207,10 @@ int lbm_create(const lbm_desc* desc, lbm_ctx** out) {
     g.gz = g.per[2] ? 0 : 1;
     g.py = g.ny + 2 * g.gy;
     g.pz = g.nz + 2 * g.gz;
+    g.pxy = (uint32_t)((size_t)g.px * g.py);
     g.slot_stride = round_up((size_t)g.px * g.py * g.pz, 64);
+    if (g.slot_stride >= (size_t(1) << 32))
+      return bail(fail(c, LBM_ERR_UNSUPPORTED, "padded grid exceeds 2^32 nodes per slot array"));
     const size_t eb = lbm::elem_bytes(desc->precision);
     if ((rc = dev_alloc(c, reinterpret_cast<char**>(&c->pop), 19 * g.slot_stride * eb,
                         "cudaMalloc(populations)")))

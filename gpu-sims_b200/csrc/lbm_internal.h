@@ -30,6 +30,7 @@ struct PhysGeom {
   int nx, ny, nz;
   int px, py, pz;      // padded extents
   int gy, gz;          // ghost offsets (0 or 1)
+  uint32_t pxy;        // px * py
   int per[3];          // periodic flags
   size_t n;            // natural node count
   size_t slot_stride;  // elements per slot array

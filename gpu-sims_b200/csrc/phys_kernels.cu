@@ -89,18 +89,23 @@ __device__ __forceinline__ float wall_term(const PhysParams& p, int x, int y, in
   return 6.0f * wf(J) * cu;
 }
 
-// Collision on shifted populations g = f - w, in place.  Returns the moments
-// (rho and the force-shifted velocity) for readback.
+// Collision on shifted populations g = f - w, in place, written per
+// opposite pair (a, b): with cu = c_a . u the equilibrium splits into an even
+// part  w (drho + rho (4.5 cu^2 - 1.5 u.u))  shared by a and b and an odd
+// part  3 w rho cu  with opposite signs, and the Guo source likewise into
+// w (9 cu (c_a.F) - 3 u.F) and 3 w (c_a.F).  Returns rho and the
+// force-shifted velocity u = (sum c g + F/2) / rho.
 template <int COLL, bool SMAG, bool FORCE>
 __device__ __forceinline__ void collide(const PhysParams& p, float (&g)[Q], float& rho_out,
                                         float& ux, float& uy, float& uz) {
-  float drho = 0.0f, jx = 0.0f, jy = 0.0f, jz = 0.0f;
-  static_for<0, Q>([&](auto I) {
-    constexpr int i = decltype(I)::value;
-    drho += g[i];
-    if (cx(i)) jx += cx(i) * g[i];
-    if (cy(i)) jy += cy(i) * g[i];
-    if (cz(i)) jz += cz(i) * g[i];
+  float drho = g[0], jx = 0.0f, jy = 0.0f, jz = 0.0f;
+  static_for<0, 9>([&](auto PI) {
+    constexpr int a = pair_a(decltype(PI)::value), b = pair_b(decltype(PI)::value);
+    const float d = g[a] - g[b];
+    drho += g[a] + g[b];
+    if (cx(a)) jx += cx(a) * d;
+    if (cy(a)) jy += cy(a) * d;
+    if (cz(a)) jz += cz(a) * d;
   });
   const float rho = 1.0f + drho;
   const float irho = 1.0f / rho;
@@ -112,30 +117,31 @@ __device__ __forceinline__ void collide(const PhysParams& p, float (&g)[Q], floa
     Fx = rho * p.accel[0];
     Fy = rho * p.accel[1];
     Fz = rho * p.accel[2];
-    ux += 0.5f * p.accel[0];
-    uy += 0.5f * p.accel[1];
-    uz += 0.5f * p.accel[2];
+    ux = fmaf(0.5f, p.accel[0], ux);
+    uy = fmaf(0.5f, p.accel[1], uy);
+    uz = fmaf(0.5f, p.accel[2], uz);
   }
   rho_out = rho;
   const float uu15 = 1.5f * (ux * ux + uy * uy + uz * uz);
+  const float uF = FORCE ? (ux * Fx + uy * Fy + uz * Fz) : 0.0f;
 
   float omega = p.omega;
   if (SMAG) {
-    // Non-equilibrium momentum flux Pi = sum c c (f - feq) and the
-    // Hou et al. (1996) effective relaxation time
+    // Non-equilibrium momentum flux Pi = sum c c (f - feq) (even in c, so
+    // pair sums suffice) and the Hou et al. (1996) effective relaxation time
     //   tau_eff = (tau + sqrt(tau^2 + 18 sqrt(2) Cs^2 |Pi| / rho)) / 2.
     float pxx = 0.f, pyy = 0.f, pzz = 0.f, pxy = 0.f, pxz = 0.f, pyz = 0.f;
-    static_for<0, Q>([&](auto I) {
-      constexpr int i = decltype(I)::value;
-      const float cu = cx(i) * ux + cy(i) * uy + cz(i) * uz;
-      const float geq = wf(i) * (drho + rho * (3.0f * cu + 4.5f * cu * cu - uu15));
-      const float ne = g[i] - geq;
-      if (cx(i)) pxx += ne;
-      if (cy(i)) pyy += ne;
-      if (cz(i)) pzz += ne;
-      if (cx(i) * cy(i)) pxy += cx(i) * cy(i) * ne;
-      if (cx(i) * cz(i)) pxz += cx(i) * cz(i) * ne;
-      if (cy(i) * cz(i)) pyz += cy(i) * cz(i) * ne;
+    static_for<0, 9>([&](auto PI) {
+      constexpr int a = pair_a(decltype(PI)::value), b = pair_b(decltype(PI)::value);
+      const float cu = cx(a) * ux + cy(a) * uy + cz(a) * uz;
+      const float even = wf(a) * (drho + rho * fmaf(4.5f * cu, cu, -uu15));
+      const float ne = (g[a] + g[b]) - 2.0f * even;
+      if (cx(a)) pxx += ne;
+      if (cy(a)) pyy += ne;
+      if (cz(a)) pzz += ne;
+      if (cx(a) * cy(a)) pxy += cx(a) * cy(a) * ne;
+      if (cx(a) * cz(a)) pxz += cx(a) * cz(a) * ne;
+      if (cy(a) * cz(a)) pyz += cy(a) * cz(a) * ne;
     });
     const float pn = sqrtf(pxx * pxx + pyy * pyy + pzz * pzz +
                            2.0f * (pxy * pxy + pxz * pxz + pyz * pyz));
@@ -143,132 +149,185 @@ __device__ __forceinline__ void collide(const PhysParams& p, float (&g)[Q], floa
     const float tau_eff = 0.5f * (p.tau + sqrtf(p.tau * p.tau + 25.455844f * cs2 * pn * irho));
     omega = 1.0f / tau_eff;
   }
-
-  if (COLL == LBM_COLL_BGK) {
-    const float fpre = 1.0f - 0.5f * omega;
-    static_for<0, Q>([&](auto I) {
-      constexpr int i = decltype(I)::value;
-      const float cu = cx(i) * ux + cy(i) * uy + cz(i) * uz;
-      const float geq = wf(i) * (drho + rho * (3.0f * cu + 4.5f * cu * cu - uu15));
-      float gn = g[i] + omega * (geq - g[i]);
-      if (FORCE) {
-        const float cF = cx(i) * Fx + cy(i) * Fy + cz(i) * Fz;
-        const float uF = ux * Fx + uy * Fy + uz * Fz;
-        gn += fpre * wf(i) * (3.0f * (cF - uF) + 9.0f * cu * cF);
-      }
-      g[i] = gn;
-    });
-  } else {
-    // TRT: omega+ = omega, omega- from the magic parameter
-    //   Lambda = (1/omega+ - 1/2)(1/omega- - 1/2).
-    const float tau_p = 1.0f / omega;
-    const float omega_m = 1.0f / (p.trt_magic / (tau_p - 0.5f) + 0.5f);
-    const float fp = 1.0f - 0.5f * omega, fm = 1.0f - 0.5f * omega_m;
-    const float uF = FORCE ? (ux * Fx + uy * Fy + uz * Fz) : 0.0f;
-    {
-      const float geq0 = wf(0) * (drho - rho * uu15);
-      float g0 = g[0] + omega * (geq0 - g[0]);
-      if (FORCE) g0 += fp * wf(0) * (-3.0f * uF);
-      g[0] = g0;
-    }
-    static_for<0, 9>([&](auto P) {
-      constexpr int a = pair_a(decltype(P)::value), b = pair_b(decltype(P)::value);
-      const float cu = cx(a) * ux + cy(a) * uy + cz(a) * uz;
-      const float eqp = wf(a) * (drho + rho * (4.5f * cu * cu - uu15));
-      const float eqm = wf(a) * rho * 3.0f * cu;
-      const float gp = 0.5f * (g[a] + g[b]), gm = 0.5f * (g[a] - g[b]);
-      const float dp = omega * (eqp - gp), dm = omega_m * (eqm - gm);
-      float na = g[a] + dp + dm, nb = g[b] + dp - dm;
-      if (FORCE) {
-        const float cF = cx(a) * Fx + cy(a) * Fy + cz(a) * Fz;
-        const float sp = fp * wf(a) * (-3.0f * uF + 9.0f * cu * cF);
-        const float sm = fm * wf(a) * 3.0f * cF;
-        na += sp + sm;
-        nb += sp - sm;
-      }
-      g[a] = na;
-      g[b] = nb;
-    });
+  // odd-part relaxation rate: BGK relaxes both parts with omega; TRT uses
+  // omega- from Lambda = (1/omega+ - 1/2)(1/omega- - 1/2).
+  const float omega_m =
+      COLL == LBM_COLL_BGK ? omega : 1.0f / (p.trt_magic / (1.0f / omega - 0.5f) + 0.5f);
+  const float fp = 1.0f - 0.5f * omega, fm = 1.0f - 0.5f * omega_m;
+  {
+    const float eq0 = wf(0) * (drho - rho * uu15);
+    float g0 = fmaf(omega, eq0 - g[0], g[0]);
+    if (FORCE) g0 = fmaf(fp * wf(0), -3.0f * uF, g0);
+    g[0] = g0;
   }
+  static_for<0, 9>([&](auto PI) {
+    constexpr int a = pair_a(decltype(PI)::value), b = pair_b(decltype(PI)::value);
+    const float cu = cx(a) * ux + cy(a) * uy + cz(a) * uz;
+    const float even = wf(a) * (drho + rho * fmaf(4.5f * cu, cu, -uu15));
+    const float odd = (3.0f * wf(a)) * rho * cu;
+    const float gp = 0.5f * (g[a] + g[b]), gm = 0.5f * (g[a] - g[b]);
+    float dp = omega * (even - gp), dm = omega_m * (odd - gm);
+    if (FORCE) {
+      const float cF = cx(a) * Fx + cy(a) * Fy + cz(a) * Fz;
+      dp = fmaf(fp * wf(a), fmaf(9.0f * cu, cF, -3.0f * uF), dp);
+      dm = fmaf(fm * (3.0f * wf(a)), cF, dm);
+    }
+    g[a] += dp + dm;
+    g[b] += dp - dm;
+  });
 }
 
+// Launch shape of the step kernel: a block is 32 x STEP_BY nodes of one
+// z-plane, so every warp covers 32 consecutive x of one row.
+constexpr int STEP_BY = 4;
+constexpr int STEP_THREADS = 32 * STEP_BY;
+constexpr unsigned FULL = 0xffffffffu;
+
+__device__ __forceinline__ uint32_t lin32(const PhysGeom& g, int x, int y, int z) {
+  return (uint32_t)x + (uint32_t)g.px * ((uint32_t)(y + g.gy) + (uint32_t)g.py * (uint32_t)(z + g.gz));
+}
+
+template <int DX, int DY, int DZ>
+__device__ __forceinline__ uint32_t lin32_fwd(const PhysGeom& g, int x, int y, int z) {
+  int xn = x + DX, yn = y + DY, zn = z + DZ;
+  if (DX != 0 && g.per[0]) xn = xn >= g.nx ? xn - g.nx : xn;
+  if (DY != 0 && g.per[1]) yn = yn >= g.ny ? yn - g.ny : (yn < 0 ? yn + g.ny : yn);
+  if (DZ != 0 && g.per[2]) zn = zn >= g.nz ? zn - g.nz : (zn < 0 ? zn + g.nz : zn);
+  return lin32(g, xn, yn, zn);
+}
+
+// Padded-index offset of n + (0, DY, DZ) (X == 0) or n + (DX, DY, DZ)
+// (X == 1) from n, periodic wrap included; w* are the per-node wrap terms.
+struct Wrap {
+  uint32_t wx, wyp, wym, wzp, wzm;
+};
+
+__device__ __forceinline__ Wrap wrap_terms(const PhysGeom& G, int x, int y, int z) {
+  Wrap w;
+  w.wx = (G.per[0] && x == G.nx - 1) ? (uint32_t)(-G.nx) : 0u;
+  w.wyp = (G.per[1] && y == G.ny - 1) ? (uint32_t)0 - (uint32_t)G.ny * (uint32_t)G.px : 0u;
+  w.wym = (G.per[1] && y == 0) ? (uint32_t)G.ny * (uint32_t)G.px : 0u;
+  w.wzp = (G.per[2] && z == G.nz - 1) ? (uint32_t)0 - (uint32_t)G.nz * G.pxy : 0u;
+  w.wzm = (G.per[2] && z == 0) ? (uint32_t)G.nz * G.pxy : 0u;
+  return w;
+}
+
+template <int DX, int DY, int DZ>
+__device__ __forceinline__ uint32_t offs(const PhysGeom& G, const Wrap& w) {
+  uint32_t o = (uint32_t)DX + (uint32_t)(DY * G.px) + (uint32_t)DZ * G.pxy;
+  if (DX > 0) o += w.wx;
+  if (DY > 0) o += w.wyp;
+  if (DY < 0) o += w.wym;
+  if (DZ > 0) o += w.wzp;
+  if (DZ < 0) o += w.wzm;
+  return o;
+}
+
+// One fused stream+collide launch.  All lanes of a warp stay converged:
+//  * the 19 slots of the streaming pattern are loaded before the flag byte
+//    is known (a solid node's slots exist, so the loads are in bounds), so a
+//    node costs one memory round trip, not two;
+//  * the five pairs whose forward vector has cx = +1 read and write slot
+//    Y at x+1.  Instead of a 4-byte-shifted warp access, every lane accesses
+//    its own aligned x and the values move one lane by warp shuffle; the
+//    last lane of a warp (or of a row) touches x+1 directly;
+//  * boundary nodes (flag bit) then re-read the bounce-back slots.
 template <int PREC, int COLL, bool SMAG, bool FORCE, bool WRITE_MOMENTS>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(STEP_THREADS, 6)
     k_phys_step(PhysParams p, int P, void* __restrict__ pop_v, const uint8_t* __restrict__ flags,
                 const uint32_t* __restrict__ links, float* __restrict__ rho_o,
                 float* __restrict__ u_o, unsigned* __restrict__ status) {
   using S = Store<PREC>;
   using T = typename S::T;
   const PhysGeom& G = p.g;
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z * blockDim.z + threadIdx.z;
-  if (x >= G.nx || y >= G.ny || z >= G.nz) return;
-  const size_t N = G.n;
-  const size_t nid = (size_t)x + (size_t)G.nx * ((size_t)y + (size_t)G.ny * (size_t)z);
-  const uint8_t fl = flags[nid];
-  if (fl & FLAG_SOLID) {
-    if (WRITE_MOMENTS) {
-      rho_o[nid] = 0.0f;
-      u_o[nid] = 0.0f;
-      u_o[N + nid] = 0.0f;
-      u_o[2 * N + nid] = 0.0f;
-    }
-    return;
-  }
+  const int lane = threadIdx.x;
+  const int y = blockIdx.y * STEP_BY + threadIdx.y;
+  if (y >= G.ny) return;  // uniform over the warp
+  const int z = blockIdx.z;
+  const int x = blockIdx.x * 32 + lane;
+  const bool valid = x < G.nx;
+  const int xc = valid ? x : G.nx - 1;  // in-bounds address for idle lanes
+  const bool edge = (lane == 31) || (x >= G.nx - 1);  // touches x+1 itself
+  const uint32_t N = (uint32_t)G.n;
+  const uint32_t nid = (uint32_t)xc + (uint32_t)G.nx * ((uint32_t)y + (uint32_t)G.ny * (uint32_t)z);
   T* pop = reinterpret_cast<T*>(pop_v);
   const size_t SS = G.slot_stride;
-  const size_t ln = lin(G, x, y, z);
-  const uint32_t L = (fl & FLAG_BOUNDARY) ? links[nid] : 0u;
-  const bool moving = p.any_moving_wall && L;
+  const uint32_t ln = lin32(G, xc, y, z);
+  const Wrap w = wrap_terms(G, xc, y, z);
 
+  const uint8_t fl = valid ? flags[nid] : FLAG_SOLID;
   float g[Q];
-  size_t lf[9];
   g[0] = S::ld(pop, ln);
   static_for<0, 9>([&](auto PI) {
     constexpr int pi = decltype(PI)::value;
     constexpr int a = pair_a(pi), b = pair_b(pi);
-    const size_t fwd = lin_fwd<cx(a), cy(a), cz(a)>(G, x, y, z);
-    lf[pi] = fwd;
+    constexpr int DX = cx(a), DY = cy(a), DZ = cz(a);
     const T* s0 = pop + (size_t)(1 + 2 * pi) * SS;
-    const T* s1 = s0 + SS;
-    const T* sP = P ? s1 : s0;   // S[P]
-    const T* sQ = P ? s0 : s1;   // S[1-P]
-    if (!L) {
-      g[a] = S::ld(sQ, ln);
-      g[b] = S::ld(sP, fwd);
+    const T* sP = P ? s0 + SS : s0;
+    const T* sQ = P ? s0 : s0 + SS;
+    g[a] = S::ld(sQ, ln);
+    if (DX == 0) {
+      g[b] = S::ld(sP, ln + offs<0, DY, DZ>(G, w));
     } else {
-      const bool blk_fwd = (L >> a) & 1u;  // n + d is a wall
-      const bool blk_bwd = (L >> b) & 1u;  // n - d is a wall
-      g[a] = blk_bwd ? S::ld(sP, ln) : S::ld(sQ, ln);
-      g[b] = blk_fwd ? S::ld(sQ, fwd) : S::ld(sP, fwd);
-      if (moving) {
-        if (blk_bwd) g[a] += wall_term<a>(p, x, y, z);
-        if (blk_fwd) g[b] += wall_term<b>(p, x, y, z);
-      }
+      const float own = S::ld(sP, ln + offs<0, DY, DZ>(G, w));
+      float nb = __shfl_down_sync(FULL, own, 1);
+      if (edge) nb = S::ld(sP, ln + offs<1, DY, DZ>(G, w));
+      g[b] = nb;
     }
   });
+
+  const bool fluid = valid && !(fl & FLAG_SOLID);
+  if (fluid && (fl & FLAG_BOUNDARY)) {
+    const uint32_t L = links[nid];
+    const bool moving = p.any_moving_wall;
+    static_for<0, 9>([&](auto PI) {
+      constexpr int pi = decltype(PI)::value;
+      constexpr int a = pair_a(pi), b = pair_b(pi);
+      const T* s0 = pop + (size_t)(1 + 2 * pi) * SS;
+      const T* sP = P ? s0 + SS : s0;
+      const T* sQ = P ? s0 : s0 + SS;
+      if ((L >> b) & 1u) {  // n - d is a wall: f_a(n) = f*_b(n) from S[P](n)
+        g[a] = S::ld(sP, ln);
+        if (moving) g[a] += wall_term<a>(p, x, y, z);
+      }
+      if ((L >> a) & 1u) {  // n + d is a wall: f_b(n) = f*_a(n) from S[1-P](n+d)
+        g[b] = S::ld(sQ, ln + offs<cx(a), cy(a), cz(a)>(G, w));
+        if (moving) g[b] += wall_term<b>(p, x, y, z);
+      }
+    });
+  }
 
   float rho, ux, uy, uz;
   collide<COLL, SMAG, FORCE>(p, g, rho, ux, uy, uz);
 
-  if (WRITE_MOMENTS) {
-    rho_o[nid] = rho;
-    u_o[nid] = ux;
-    u_o[N + nid] = uy;
-    u_o[2 * N + nid] = uz;
-    if (!(rho > 0.0f) || !isfinite(rho) || !isfinite(ux) || !isfinite(uy) || !isfinite(uz))
+  if (WRITE_MOMENTS && valid) {
+    const bool s = !fluid;
+    rho_o[nid] = s ? 0.0f : rho;
+    u_o[nid] = s ? 0.0f : ux;
+    u_o[N + nid] = s ? 0.0f : uy;
+    u_o[2 * N + nid] = s ? 0.0f : uz;
+    if (fluid && (!(rho > 0.0f) || !isfinite(rho) || !isfinite(ux) || !isfinite(uy) || !isfinite(uz)))
       atomicOr(status, 1u);
   }
 
-  S::st(pop, ln, g[0]);
+  if (fluid) S::st(pop, ln, g[0]);
+  const bool pass = fluid && !edge;  // this lane's Y value is stored by lane+1
   static_for<0, 9>([&](auto PI) {
     constexpr int pi = decltype(PI)::value;
     constexpr int a = pair_a(pi), b = pair_b(pi);
+    constexpr int DX = cx(a), DY = cy(a), DZ = cz(a);
     T* s0 = pop + (size_t)(1 + 2 * pi) * SS;
-    T* s1 = s0 + SS;
-    S::st(P ? s1 : s0, lf[pi], g[a]);  // f*_a -> Y = S[P](n + d)
-    S::st(P ? s0 : s1, ln, g[b]);      // f*_b -> X = S[1-P](n)
+    T* sP = P ? s0 + SS : s0;
+    T* sQ = P ? s0 : s0 + SS;
+    if (fluid) S::st(sQ, ln, g[b]);  // f*_b -> X = S[1-P](n)
+    if (DX == 0) {
+      if (fluid) S::st(sP, ln + offs<0, DY, DZ>(G, w), g[a]);  // f*_a -> Y = S[P](n+d)
+    } else {
+      const float from_left = __shfl_up_sync(FULL, g[a], 1);
+      const bool left_ok = __shfl_up_sync(FULL, pass, 1) && lane > 0;
+      if (left_ok) S::st(sP, ln + offs<0, DY, DZ>(G, w), from_left);
+      if (fluid && edge) S::st(sP, ln + offs<1, DY, DZ>(G, w), g[a]);
+    }
   });
 }
 
@@ -397,11 +456,13 @@ dim3 phys_grid(const PhysGeom& g) {
 template <int PREC, int COLL, bool SMAG, bool FORCE>
 cudaError_t launch_step(const Ctx& c, int P, bool wm, cudaStream_t s) {
   const PhysGeom& G = c.pp.g;
+  const dim3 blk(32, STEP_BY, 1);
+  const dim3 grd((G.nx + 31) / 32, (G.ny + STEP_BY - 1) / STEP_BY, G.nz);
   if (wm)
-    k_phys_step<PREC, COLL, SMAG, FORCE, true><<<phys_grid(G), phys_block(), 0, s>>>(
+    k_phys_step<PREC, COLL, SMAG, FORCE, true><<<grd, blk, 0, s>>>(
         c.pp, P, c.pop, c.flags, c.links, c.rho, c.u, c.status);
   else
-    k_phys_step<PREC, COLL, SMAG, FORCE, false><<<phys_grid(G), phys_block(), 0, s>>>(
+    k_phys_step<PREC, COLL, SMAG, FORCE, false><<<grd, blk, 0, s>>>(
         c.pp, P, c.pop, c.flags, c.links, c.rho, c.u, c.status);
   return cudaGetLastError();
 }
