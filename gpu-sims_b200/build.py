@@ -46,8 +46,15 @@ def _stale(obj: Path, src: Path) -> bool:
     return any(d.stat().st_mtime > obj.stat().st_mtime for d in deps)
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    BUILD.mkdir(exist_ok=True)
+def build(force: bool = False, verbose: bool = False, out: Path | None = None,
+          build_dir: Path | None = None, defines: list[str] | None = None) -> Path:
+    """Compiles every source in csrc/ and links the shared library.  `out`,
+    `build_dir` and `defines` (-D flags) allow variant builds elsewhere."""
+    global BUILD, OUT
+    BUILD = build_dir or BUILD
+    OUT = out or OUT
+    extra = [f"-D{d}" for d in (defines or [])]
+    BUILD.mkdir(parents=True, exist_ok=True)
     cc = nvcc()
     objs = []
     for src in sources():
@@ -55,9 +62,9 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         objs.append(obj)
         if not force and not _stale(obj, src):
             continue
-        cmd = [cc, "-c", str(src), "-o", str(obj)] + CUDA_FLAGS + HOST_EXTRA.get(src.name, [])
+        cmd = [cc, "-c", str(src), "-o", str(obj)] + CUDA_FLAGS + extra + HOST_EXTRA.get(src.name, [])
         if src.suffix == ".cpp":
-            cmd = [cc, "-x", "cu", "-c", str(src), "-o", str(obj)] + CUDA_FLAGS + HOST_EXTRA.get(src.name, [])
+            cmd = [cc, "-x", "cu", "-c", str(src), "-o", str(obj)] + CUDA_FLAGS + extra + HOST_EXTRA.get(src.name, [])
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -33,14 +33,23 @@ namespace lbm {
 constexpr float F16_SCALE = 4096.0f;
 constexpr float F16_INV_SCALE = 1.0f / 4096.0f;
 
+// Storage traits.  The step kernel works in "storage units" v = SC * g
+// (SC = 1 for fp32 and bf16, 2^12 for fp16) so that loads and stores need no
+// rescaling; ld/st convert to plain g for init and population transfer.
 template <int PREC> struct Store;
 template <> struct Store<LBM_PREC_F32> {
   using T = float;
+  static constexpr float SC = 1.0f, INV = 1.0f;
+  static __device__ __forceinline__ float raw_ld(const T* p, uint32_t i) { return p[i]; }
+  static __device__ __forceinline__ void raw_st(T* p, uint32_t i, float v) { p[i] = v; }
   static __device__ __forceinline__ float ld(const T* p, size_t i) { return p[i]; }
   static __device__ __forceinline__ void st(T* p, size_t i, float v) { p[i] = v; }
 };
 template <> struct Store<LBM_PREC_F16S> {
   using T = __half;
+  static constexpr float SC = F16_SCALE, INV = F16_INV_SCALE;
+  static __device__ __forceinline__ float raw_ld(const T* p, uint32_t i) { return __half2float(p[i]); }
+  static __device__ __forceinline__ void raw_st(T* p, uint32_t i, float v) { p[i] = __float2half_rn(v); }
   static __device__ __forceinline__ float ld(const T* p, size_t i) {
     return __half2float(p[i]) * F16_INV_SCALE;
   }
@@ -50,6 +59,9 @@ template <> struct Store<LBM_PREC_F16S> {
 };
 template <> struct Store<LBM_PREC_BF16S> {
   using T = __nv_bfloat16;
+  static constexpr float SC = 1.0f, INV = 1.0f;
+  static __device__ __forceinline__ float raw_ld(const T* p, uint32_t i) { return __bfloat162float(p[i]); }
+  static __device__ __forceinline__ void raw_st(T* p, uint32_t i, float v) { p[i] = __float2bfloat16_rn(v); }
   static __device__ __forceinline__ float ld(const T* p, size_t i) { return __bfloat162float(p[i]); }
   static __device__ __forceinline__ void st(T* p, size_t i, float v) { p[i] = __float2bfloat16_rn(v); }
 };
@@ -89,52 +101,55 @@ __device__ __forceinline__ float wall_term(const PhysParams& p, int x, int y, in
   return 6.0f * wf(J) * cu;
 }
 
-// Collision on shifted populations g = f - w, in place, written per
-// opposite pair (a, b): with cu = c_a . u the equilibrium splits into an even
-// part  w (drho + rho (4.5 cu^2 - 1.5 u.u))  shared by a and b and an odd
-// part  3 w rho cu  with opposite signs, and the Guo source likewise into
-// w (9 cu (c_a.F) - 3 u.F) and 3 w (c_a.F).  Returns rho and the
-// force-shifted velocity u = (sum c g + F/2) / rho.
-template <int COLL, bool SMAG, bool FORCE>
+// Collision on shifted populations in storage units v = SC (f - w), in
+// place, written per opposite pair (a, b): with cu = c_a . u the equilibrium
+// splits into an even part  w (drho + rho (4.5 cu^2 - 1.5 u.u))  shared by a
+// and b and an odd part  3 w rho cu  with opposite signs; the Guo source
+// splits into  w rho (9 cu (c_a.g) - 3 u.g)  and  3 w rho (c_a.g)  (g the
+// body acceleration, F = rho g).  BGK relaxes both parts with omega; TRT the
+// odd part with omega-, from Lambda = (1/omega - 1/2)(1/omega- - 1/2):
+//   v_a' = (1 - h) v_a - k v_b + E + O,   v_b' = (1 - h) v_b - k v_a + E - O
+// with h = (omega + omega-)/2, k = (omega - omega-)/2, E = omega even +
+// (1 - omega/2) even source, O = omega- odd + (1 - omega-/2) odd source.
+// Returns rho and the force-shifted velocity u = (sum c f + F/2) / rho.
+template <int COLL, bool SMAG, bool FORCE, int PREC>
 __device__ __forceinline__ void collide(const PhysParams& p, float (&g)[Q], float& rho_out,
                                         float& ux, float& uy, float& uz) {
-  float drho = g[0], jx = 0.0f, jy = 0.0f, jz = 0.0f;
+  constexpr float SC = Store<PREC>::SC, INV = Store<PREC>::INV;
+  constexpr float WF = 1.0f / 18.0f, WE = 1.0f / 36.0f, W0 = 1.0f / 3.0f;
+  float drs = g[0], jx = 0.0f, jy = 0.0f, jz = 0.0f;  // sums in storage units
   static_for<0, 9>([&](auto PI) {
     constexpr int a = pair_a(decltype(PI)::value), b = pair_b(decltype(PI)::value);
     const float d = g[a] - g[b];
-    drho += g[a] + g[b];
+    drs += g[a] + g[b];
     if (cx(a)) jx += cx(a) * d;
     if (cy(a)) jy += cy(a) * d;
     if (cz(a)) jz += cz(a) * d;
   });
-  const float rho = 1.0f + drho;
-  const float irho = 1.0f / rho;
-  ux = jx * irho;
-  uy = jy * irho;
-  uz = jz * irho;
-  float Fx = 0.f, Fy = 0.f, Fz = 0.f;
+  const float rho = fmaf(drs, INV, 1.0f);
+  const float js = INV / rho;
+  ux = jx * js;
+  uy = jy * js;
+  uz = jz * js;
   if (FORCE) {
-    Fx = rho * p.accel[0];
-    Fy = rho * p.accel[1];
-    Fz = rho * p.accel[2];
     ux = fmaf(0.5f, p.accel[0], ux);
     uy = fmaf(0.5f, p.accel[1], uy);
     uz = fmaf(0.5f, p.accel[2], uz);
   }
   rho_out = rho;
   const float uu15 = 1.5f * (ux * ux + uy * uy + uz * uz);
-  const float uF = FORCE ? (ux * Fx + uy * Fy + uz * Fz) : 0.0f;
+  const float sr = SC * rho;
 
   float omega = p.omega;
   if (SMAG) {
-    // Non-equilibrium momentum flux Pi = sum c c (f - feq) (even in c, so
-    // pair sums suffice) and the Hou et al. (1996) effective relaxation time
+    // Pi = sum c c (f - feq) (even in c: pair sums suffice); Hou et al. (1996)
     //   tau_eff = (tau + sqrt(tau^2 + 18 sqrt(2) Cs^2 |Pi| / rho)) / 2.
     float pxx = 0.f, pyy = 0.f, pzz = 0.f, pxy = 0.f, pxz = 0.f, pyz = 0.f;
     static_for<0, 9>([&](auto PI) {
       constexpr int a = pair_a(decltype(PI)::value), b = pair_b(decltype(PI)::value);
+      constexpr float w = wf(a);
       const float cu = cx(a) * ux + cy(a) * uy + cz(a) * uz;
-      const float even = wf(a) * (drho + rho * fmaf(4.5f * cu, cu, -uu15));
+      const float even = fmaf(w * sr, fmaf(4.5f * cu, cu, -uu15), w * drs);
       const float ne = (g[a] + g[b]) - 2.0f * even;
       if (cx(a)) pxx += ne;
       if (cy(a)) pyy += ne;
@@ -143,43 +158,66 @@ __device__ __forceinline__ void collide(const PhysParams& p, float (&g)[Q], floa
       if (cx(a) * cz(a)) pxz += cx(a) * cz(a) * ne;
       if (cy(a) * cz(a)) pyz += cy(a) * cz(a) * ne;
     });
-    const float pn = sqrtf(pxx * pxx + pyy * pyy + pzz * pzz +
-                           2.0f * (pxy * pxy + pxz * pxz + pyz * pyz));
+    const float pn = INV * sqrtf(pxx * pxx + pyy * pyy + pzz * pzz +
+                                 2.0f * (pxy * pxy + pxz * pxz + pyz * pyz));
     const float cs2 = p.smag_cs * p.smag_cs;
-    const float tau_eff = 0.5f * (p.tau + sqrtf(p.tau * p.tau + 25.455844f * cs2 * pn * irho));
+    const float tau_eff = 0.5f * (p.tau + sqrtf(fmaf(p.tau, p.tau, 25.455844f * cs2 * pn / rho)));
     omega = 1.0f / tau_eff;
   }
-  // odd-part relaxation rate: BGK relaxes both parts with omega; TRT uses
-  // omega- from Lambda = (1/omega+ - 1/2)(1/omega- - 1/2).
   const float omega_m =
       COLL == LBM_COLL_BGK ? omega : 1.0f / (p.trt_magic / (1.0f / omega - 0.5f) + 0.5f);
-  const float fp = 1.0f - 0.5f * omega, fm = 1.0f - 0.5f * omega_m;
+  const float h = 0.5f * (omega + omega_m), k = 0.5f * (omega - omega_m);
+  const float c1 = 1.0f - h;
+  // per weight class: omega w SC rho, omega w drs, 3 omega- w SC rho, source factors
+  const float erF = omega * WF * sr, erE = omega * WE * sr;
+  const float edF = omega * WF * drs, edE = omega * WE * drs;
+  const float orF = 3.0f * omega_m * WF * sr, orE = 3.0f * omega_m * WE * sr;
+  float ua3 = 0.f, ksF = 0.f, ksE = 0.f, kaF = 0.f, kaE = 0.f;
+  if (FORCE) {
+    ua3 = 3.0f * (ux * p.accel[0] + uy * p.accel[1] + uz * p.accel[2]);
+    const float fp = 1.0f - 0.5f * omega, fm = 1.0f - 0.5f * omega_m;
+    ksF = fp * WF * sr;
+    ksE = fp * WE * sr;
+    kaF = 3.0f * fm * WF * sr;
+    kaE = 3.0f * fm * WE * sr;
+  }
   {
-    const float eq0 = wf(0) * (drho - rho * uu15);
-    float g0 = fmaf(omega, eq0 - g[0], g[0]);
-    if (FORCE) g0 = fmaf(fp * wf(0), -3.0f * uF, g0);
-    g[0] = g0;
+    float e0 = fmaf(-omega * W0 * sr, uu15, omega * W0 * drs);
+    if (FORCE) e0 = fmaf(-(1.0f - 0.5f * omega) * W0 * sr, ua3, e0);
+    g[0] = fmaf(1.0f - omega, g[0], e0);
   }
   static_for<0, 9>([&](auto PI) {
     constexpr int a = pair_a(decltype(PI)::value), b = pair_b(decltype(PI)::value);
+    constexpr bool face = (a <= 6);
     const float cu = cx(a) * ux + cy(a) * uy + cz(a) * uz;
-    const float even = wf(a) * (drho + rho * fmaf(4.5f * cu, cu, -uu15));
-    const float odd = (3.0f * wf(a)) * rho * cu;
-    const float gp = 0.5f * (g[a] + g[b]), gm = 0.5f * (g[a] - g[b]);
-    float dp = omega * (even - gp), dm = omega_m * (odd - gm);
+    const float t = fmaf(4.5f * cu, cu, -uu15);
+    float E = fmaf(face ? erF : erE, t, face ? edF : edE);
+    float O = (face ? orF : orE) * cu;
     if (FORCE) {
-      const float cF = cx(a) * Fx + cy(a) * Fy + cz(a) * Fz;
-      dp = fmaf(fp * wf(a), fmaf(9.0f * cu, cF, -3.0f * uF), dp);
-      dm = fmaf(fm * (3.0f * wf(a)), cF, dm);
+      const float ca = cx(a) * p.accel[0] + cy(a) * p.accel[1] + cz(a) * p.accel[2];
+      E = fmaf(face ? ksF : ksE, fmaf(9.0f * ca, cu, -ua3), E);
+      O = fmaf(face ? kaF : kaE, ca, O);
     }
-    g[a] += dp + dm;
-    g[b] += dp - dm;
+    const float ga = g[a], gb = g[b];
+    if (COLL == LBM_COLL_BGK) {
+      g[a] = fmaf(c1, ga, E + O);
+      g[b] = fmaf(c1, gb, E - O);
+    } else {
+      g[a] = fmaf(c1, ga, fmaf(-k, gb, E + O));
+      g[b] = fmaf(c1, gb, fmaf(-k, ga, E - O));
+    }
   });
 }
 
 // Launch shape of the step kernel: a block is 32 x STEP_BY nodes of one
 // z-plane, so every warp covers 32 consecutive x of one row.
-constexpr int STEP_BY = 4;
+#ifndef LBM_STEP_BY
+#define LBM_STEP_BY 4
+#endif
+#ifndef LBM_STEP_MINB
+#define LBM_STEP_MINB 6
+#endif
+constexpr int STEP_BY = LBM_STEP_BY;
 constexpr int STEP_THREADS = 32 * STEP_BY;
 constexpr unsigned FULL = 0xffffffffu;
 
@@ -232,9 +270,9 @@ __device__ __forceinline__ uint32_t offs(const PhysGeom& G, const Wrap& w) {
 //    its own aligned x and the values move one lane by warp shuffle; the
 //    last lane of a warp (or of a row) touches x+1 directly;
 //  * boundary nodes (flag bit) then re-read the bounce-back slots.
-template <int PREC, int COLL, bool SMAG, bool FORCE, bool WRITE_MOMENTS>
-__global__ void __launch_bounds__(STEP_THREADS, 6)
-    k_phys_step(PhysParams p, int P, void* __restrict__ pop_v, const uint8_t* __restrict__ flags,
+template <int PREC, int COLL, bool SMAG, bool FORCE, bool WRITE_MOMENTS, int P>
+__global__ void __launch_bounds__(STEP_THREADS, LBM_STEP_MINB)
+    k_phys_step(PhysParams p, void* __restrict__ pop_v, const uint8_t* __restrict__ flags,
                 const uint32_t* __restrict__ links, float* __restrict__ rho_o,
                 float* __restrict__ u_o, unsigned* __restrict__ status) {
   using S = Store<PREC>;
@@ -257,7 +295,7 @@ __global__ void __launch_bounds__(STEP_THREADS, 6)
 
   const uint8_t fl = valid ? flags[nid] : FLAG_SOLID;
   float g[Q];
-  g[0] = S::ld(pop, ln);
+  g[0] = S::raw_ld(pop, ln);
   static_for<0, 9>([&](auto PI) {
     constexpr int pi = decltype(PI)::value;
     constexpr int a = pair_a(pi), b = pair_b(pi);
@@ -265,13 +303,13 @@ __global__ void __launch_bounds__(STEP_THREADS, 6)
     const T* s0 = pop + (size_t)(1 + 2 * pi) * SS;
     const T* sP = P ? s0 + SS : s0;
     const T* sQ = P ? s0 : s0 + SS;
-    g[a] = S::ld(sQ, ln);
+    g[a] = S::raw_ld(sQ, ln);
     if (DX == 0) {
-      g[b] = S::ld(sP, ln + offs<0, DY, DZ>(G, w));
+      g[b] = S::raw_ld(sP, ln + offs<0, DY, DZ>(G, w));
     } else {
-      const float own = S::ld(sP, ln + offs<0, DY, DZ>(G, w));
+      const float own = S::raw_ld(sP, ln + offs<0, DY, DZ>(G, w));
       float nb = __shfl_down_sync(FULL, own, 1);
-      if (edge) nb = S::ld(sP, ln + offs<1, DY, DZ>(G, w));
+      if (edge) nb = S::raw_ld(sP, ln + offs<1, DY, DZ>(G, w));
       g[b] = nb;
     }
   });
@@ -287,18 +325,18 @@ __global__ void __launch_bounds__(STEP_THREADS, 6)
       const T* sP = P ? s0 + SS : s0;
       const T* sQ = P ? s0 : s0 + SS;
       if ((L >> b) & 1u) {  // n - d is a wall: f_a(n) = f*_b(n) from S[P](n)
-        g[a] = S::ld(sP, ln);
-        if (moving) g[a] += wall_term<a>(p, x, y, z);
+        g[a] = S::raw_ld(sP, ln);
+        if (moving) g[a] = fmaf(S::SC, wall_term<a>(p, x, y, z), g[a]);
       }
       if ((L >> a) & 1u) {  // n + d is a wall: f_b(n) = f*_a(n) from S[1-P](n+d)
-        g[b] = S::ld(sQ, ln + offs<cx(a), cy(a), cz(a)>(G, w));
-        if (moving) g[b] += wall_term<b>(p, x, y, z);
+        g[b] = S::raw_ld(sQ, ln + offs<cx(a), cy(a), cz(a)>(G, w));
+        if (moving) g[b] = fmaf(S::SC, wall_term<b>(p, x, y, z), g[b]);
       }
     });
   }
 
   float rho, ux, uy, uz;
-  collide<COLL, SMAG, FORCE>(p, g, rho, ux, uy, uz);
+  collide<COLL, SMAG, FORCE, PREC>(p, g, rho, ux, uy, uz);
 
   if (WRITE_MOMENTS && valid) {
     const bool s = !fluid;
@@ -310,7 +348,7 @@ __global__ void __launch_bounds__(STEP_THREADS, 6)
       atomicOr(status, 1u);
   }
 
-  if (fluid) S::st(pop, ln, g[0]);
+  if (fluid) S::raw_st(pop, ln, g[0]);
   const bool pass = fluid && !edge;  // this lane's Y value is stored by lane+1
   static_for<0, 9>([&](auto PI) {
     constexpr int pi = decltype(PI)::value;
@@ -319,14 +357,14 @@ __global__ void __launch_bounds__(STEP_THREADS, 6)
     T* s0 = pop + (size_t)(1 + 2 * pi) * SS;
     T* sP = P ? s0 + SS : s0;
     T* sQ = P ? s0 : s0 + SS;
-    if (fluid) S::st(sQ, ln, g[b]);  // f*_b -> X = S[1-P](n)
+    if (fluid) S::raw_st(sQ, ln, g[b]);  // f*_b -> X = S[1-P](n)
     if (DX == 0) {
-      if (fluid) S::st(sP, ln + offs<0, DY, DZ>(G, w), g[a]);  // f*_a -> Y = S[P](n+d)
+      if (fluid) S::raw_st(sP, ln + offs<0, DY, DZ>(G, w), g[a]);  // f*_a -> Y = S[P](n+d)
     } else {
       const float from_left = __shfl_up_sync(FULL, g[a], 1);
       const bool left_ok = __shfl_up_sync(FULL, pass, 1) && lane > 0;
-      if (left_ok) S::st(sP, ln + offs<0, DY, DZ>(G, w), from_left);
-      if (fluid && edge) S::st(sP, ln + offs<1, DY, DZ>(G, w), g[a]);
+      if (left_ok) S::raw_st(sP, ln + offs<0, DY, DZ>(G, w), from_left);
+      if (fluid && edge) S::raw_st(sP, ln + offs<1, DY, DZ>(G, w), g[a]);
     }
   });
 }
@@ -458,12 +496,15 @@ cudaError_t launch_step(const Ctx& c, int P, bool wm, cudaStream_t s) {
   const PhysGeom& G = c.pp.g;
   const dim3 blk(32, STEP_BY, 1);
   const dim3 grd((G.nx + 31) / 32, (G.ny + STEP_BY - 1) / STEP_BY, G.nz);
-  if (wm)
-    k_phys_step<PREC, COLL, SMAG, FORCE, true><<<grd, blk, 0, s>>>(
-        c.pp, P, c.pop, c.flags, c.links, c.rho, c.u, c.status);
-  else
-    k_phys_step<PREC, COLL, SMAG, FORCE, false><<<grd, blk, 0, s>>>(
-        c.pp, P, c.pop, c.flags, c.links, c.rho, c.u, c.status);
+#define LBM_STEP_LAUNCH(WM, PAR)                                          \
+  k_phys_step<PREC, COLL, SMAG, FORCE, WM, PAR><<<grd, blk, 0, s>>>(      \
+      c.pp, c.pop, c.flags, c.links, c.rho, c.u, c.status)
+  if (wm) {
+    if (P) LBM_STEP_LAUNCH(true, 1); else LBM_STEP_LAUNCH(true, 0);
+  } else {
+    if (P) LBM_STEP_LAUNCH(false, 1); else LBM_STEP_LAUNCH(false, 0);
+  }
+#undef LBM_STEP_LAUNCH
   return cudaGetLastError();
 }
 
