@@ -129,6 +129,8 @@ size_t u_bytes(int fmt) {
 
 namespace lbm {
 
+void set_thread_error(const char* msg) { g_thread_err = msg; }
+
 size_t elem_bytes(int precision) { return precision == LBM_PREC_F32 ? 4 : 2; }
 
 double bytes_per_node(const lbm_desc& d) {

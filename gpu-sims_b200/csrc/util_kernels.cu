@@ -37,6 +37,8 @@ __global__ void __launch_bounds__(256)
   flags[nid] = solid ? FLAG_SOLID : ((L >> 1) ? FLAG_BOUNDARY : 0);
 }
 
+}  // namespace
+
 // Conservation sums in fp64: each block reduces with warp shuffles, writes
 // its partials; a single block then adds the partials in a fixed order, so
 // the result does not depend on scheduling.
@@ -78,6 +80,8 @@ __global__ void k_cons_final(const double* __restrict__ partials, int nblk, doub
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
   if (lane == 0) out[k] = v;
 }
+
+namespace {
 
 __global__ void k_planes_to_fmt(const float* __restrict__ u, size_t n, int fmt, void* __restrict__ out) {
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -149,3 +153,88 @@ cudaError_t u_format_to_planes(const void* in, size_t n, int fmt, float* u, cuda
 }
 
 }  // namespace lbm
+
+// ---------------------------------------------------------------------------
+// Conservation sums without any allocation.
+//
+// For callers that must not allocate device memory: a viewer's frame loop
+// that cannot afford the device-wide synchronisation cudaMalloc/cudaFree
+// imply, or a host application whose memory arena already owns the whole
+// device budget.  The two reduction kernels above are reused unchanged; their
+// block partials and the four sums live in a file-scope __device__ array that
+// every GPU loading this library holds until the process exits.
+//
+// In host code `g_noalloc_scratch` names a host-side shadow, not device
+// memory, so its device address is looked up once per device with
+// cudaGetSymbolAddress (with that device current) and the kernels receive
+// that address.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace lbm {
+void set_thread_error(const char* msg);
+}
+
+namespace {
+constexpr int kNoAllocMaxBlocks = 4096;                 // partial-sum slots per quantity
+constexpr size_t kNoAllocNodesPerBlock = 8192;          // 256 threads x 32 nodes
+constexpr size_t kNoAllocMaxNodes = kNoAllocMaxBlocks * kNoAllocNodesPerBlock;  // 33,554,432
+constexpr int kNoAllocMaxDevices = 64;
+// 4 x 4096 partials + 4 sums, fp64: 131,104 bytes per device.
+static __device__ __align__(256) double g_noalloc_scratch[4 * kNoAllocMaxBlocks + 4];
+std::mutex g_noalloc_mu;
+double* g_noalloc_addr[kNoAllocMaxDevices] = {};
+}  // namespace
+
+extern "C" LBM_API int lbm_conservation_noalloc(const float* d_rho, const float* d_u, size_t n,
+                                                double out[4], void* stream) {
+  if (!d_rho || !d_u || !out || n == 0) {
+    lbm::set_thread_error("lbm_conservation_noalloc: d_rho, d_u and out must be non-NULL and n > 0");
+    return LBM_ERR_INVALID_ARG;
+  }
+  if (n > kNoAllocMaxNodes) {
+    lbm::set_thread_error("lbm_conservation_noalloc: n exceeds the 33554432-node limit of its static "
+                          "scratch; use lbm_conservation");
+    return LBM_ERR_INVALID_ARG;
+  }
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    lbm::set_thread_error("lbm_conservation_noalloc: no current CUDA device");
+    return LBM_ERR_NO_DEVICE;
+  }
+  if (dev < 0 || dev >= kNoAllocMaxDevices) {
+    lbm::set_thread_error("lbm_conservation_noalloc: device ordinal above 63");
+    return LBM_ERR_UNSUPPORTED;
+  }
+  double* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+      void* p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess || !p) {
+        cudaGetLastError();
+        lbm::set_thread_error("lbm_conservation_noalloc: cudaGetSymbolAddress failed");
+        return LBM_ERR_CUDA;
+      }
+      g_noalloc_addr[dev] = static_cast<double*>(p);
+    }
+    scratch = g_noalloc_addr[dev];
+  }
+  // Every partial the final kernel reads is written first by its block, and
+  // the sums are overwritten, so nothing needs clearing between calls.
+  const int nblk = (int)((n + kNoAllocNodesPerBlock - 1) / kNoAllocNodesPerBlock);
+  double* sums = scratch + 4 * kNoAllocMaxBlocks;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  lbm::k_cons_partials<<<nblk, lbm::CONS_THREADS, 0, s>>>(n, d_rho, d_u, scratch, nblk);
+  lbm::k_cons_final<<<1, 128, 0, s>>>(scratch, nblk, sums);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, sums, 4 * sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    lbm::set_thread_error(cudaGetErrorString(e));
+    return LBM_ERR_CUDA;
+  }
+  return LBM_OK;
+}

@@ -89,6 +89,7 @@ _SIGS = {
     "lbm_read_moments": (C.c_int, [_P, _P, _P, C.c_int]),
     "lbm_device_moments": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P)]),
     "lbm_conservation": (C.c_int, [_P, C.POINTER(C.c_double)]),
+    "lbm_conservation_noalloc": (C.c_int, [_P, _P, C.c_size_t, C.POINTER(C.c_double), _P]),
     "lbm_read_populations": (C.c_int, [_P, _P, C.c_size_t]),
     "lbm_write_populations": (C.c_int, [_P, _P, C.c_size_t]),
     "lbm_get_info": (C.c_int, [_P, C.POINTER(Info)]),

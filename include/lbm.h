@@ -186,6 +186,22 @@ LBM_API int lbm_get_info(lbm_ctx* ctx, lbm_info* info);
  * NULL).  Never NULL. */
 LBM_API const char* lbm_last_error(lbm_ctx* ctx);
 
+/* Conservation sums of moment fields the caller already holds on the device
+ * (d_rho float[n], d_u float[3][n] planes, e.g. from lbm_device_moments),
+ * written to host out[4] as lbm_conservation does, but with no device
+ * allocation at all.  This entry point has no counterpart in the reference.
+ * It is for callers that may not allocate: a frame loop that cannot stall on
+ * the device-wide synchronisation of cudaMalloc/cudaFree, or a host whose
+ * memory arena owns the whole device budget.  Its scratch is a static
+ * 131,104-byte device array that every GPU loading the library keeps until
+ * exit; n is limited to 33,554,432 nodes (LBM_ERR_INVALID_ARG beyond).  The
+ * first call on a device looks the array's address up for that device, so
+ * make that first call before any stream capture.  All calls share the one
+ * array: calls that overlap on the GPU race.  Runs on `stream` (NULL = the
+ * legacy default stream) and synchronises it. */
+LBM_API int lbm_conservation_noalloc(const float* d_rho, const float* d_u, size_t n,
+                                     double out[4], void* stream);
+
 /* ---- host-side helpers (no GPU needed) --------------------------------- */
 
 /* D3Q19 tables in the reference's direction order
