@@ -39,6 +39,7 @@ TAU, ACCEL, NOISE, SEED = 0.55, (1e-6, 0.0, 0.0), 1e-4, 1234
 WORKLOAD = ("channel 512x128x128 D3Q19 BGK, x-periodic, body force g=1e-6 (x), half-way "
             "bounce-back y/z walls, sphere r=16 at (128,64,64), tau=0.55")
 METRIC = "D3Q19 MLUPS (channel 512x128x128, fp32 BGK)"
+REF_TIER = (256, 128, 128)
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -230,7 +231,7 @@ def run_ours(args, world, rank, local):
     n = mask.size
     peak, peak_kind = peak_hbm()
 
-    def device_run(precision: int):
+    def make_phys(precision: int):
         d = lbm.default_desc(nx=SHAPE[0], ny=SHAPE[1], nz=SHAPE[2], mode=lbm.MODE_PHYSICS,
                              precision=precision, collision=lbm.COLL_BGK, periodic=(1, 0, 0),
                              tau=TAU, body_accel=ACCEL)
@@ -238,6 +239,20 @@ def run_ours(args, world, rank, local):
         lat.set_stream(stream.cuda_stream)
         lat.set_flags(mask)
         lat.init_from_moments(rho, u)
+        return lat
+
+    def make_ref_tier():
+        """Reference mode on the reference's own desktop tier and default
+        preset (256x128x128, NACA0012 at 4 deg, |u| 0.04, tau 0.6;
+        src/main.cpp:103-135), through apply_preset."""
+        lat = lbm.Lattice(lbm.preset_desc(0, *REF_TIER))
+        lat.set_stream(stream.cuda_stream)
+        lbm.apply_preset(lat, 0)
+        return lat
+
+    def device_run(make):
+        lat = make()
+        nodes = lat.n
         bpn = lat.info().bytes_per_node
         lat.step(max(args.warmup, 3))
         barrier()
@@ -251,9 +266,10 @@ def run_ours(args, world, rank, local):
         lat.sync()
         lat.close()
         per_launch = ms / 1e3 / args.steps
-        mlups = world * n * args.steps / (ms / 1e3) / 1e6
-        achieved = n * bpn / per_launch / 1e9
-        return mlups, ms, bpn, achieved, clk.summary()
+        return {"value": world * nodes * args.steps / (ms / 1e3) / 1e6, "unit": "MLUPS",
+                "ms_per_step": ms / args.steps, "bytes_per_node": bpn,
+                "achieved_gbs": nodes * bpn / per_launch / 1e9,
+                "frac": nodes * bpn / per_launch / 1e9 / peak, "clocks": clk.summary()}
 
     def e2e_run(precision: int):
         """Through the C ABI with host buffers: upload flags and initial
@@ -293,35 +309,48 @@ def run_ours(args, world, rank, local):
                         "lbm_step(1) and a read of the fp64 conservation sums, final rho/u read "
                         "to pinned host memory"}
 
-    mlups, ms, bpn, achieved, clocks = device_run(lbm.PREC_F32)
-    h_mlups, h_ms, h_bpn, h_ach, h_clocks = device_run(lbm.PREC_F16S)
-    e2e = e2e_run(lbm.PREC_F32)
+    runs = {}
+    want = args.variant
+    if want in ("all", "f32"):
+        runs["f32"] = device_run(lambda: make_phys(lbm.PREC_F32))
+    if want in ("all", "f16s"):
+        runs["f16s"] = device_run(lambda: make_phys(lbm.PREC_F16S))
+    if want in ("all", "bf16s"):
+        runs["bf16s"] = device_run(lambda: make_phys(lbm.PREC_BF16S))
+    if want in ("all", "ref"):
+        runs["reference_mode_desktop_tier"] = device_run(make_ref_tier)
+    e2e = e2e_run(lbm.PREC_F32) if (want in ("all", "f32") and not args.no_e2e) else None
     cpu = cpu_baseline_sample() if (rank == 0 and world == 1 and not args.no_cpu) else None
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     if rank != 0:
         return 0
-    traffic = ncu_traffic("lbm_step_channel_fp32")
+    head_key = "f32" if "f32" in runs else next(iter(runs))
+    head = runs.pop(head_key)
+    if "f32" == head_key:
+        for k in ("f16s", "bf16s"):
+            if k in runs:
+                runs[k]["speedup_vs_f32"] = runs[k]["value"] / head["value"]
+    traffic = ncu_traffic("lbm_step_channel_fp32") if head_key == "f32" else None
     line = {
-        "metric": METRIC, "value": mlups, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
-        "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "nodes": n, "precision": "fp32 populations (f - w)",
+        "metric": METRIC, "value": head["value"], "unit": "MLUPS", "n_gpus": world,
+        "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": head["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if head_key == "f32" else head_key, "data": "synthetic",
+        "config": {"workload": WORKLOAD, "nodes": n, "precision": f"{head_key} populations (f - w)",
                    "layout": "esoteric pull, one population store",
                    "l2": "inputs larger than L2 (populations %.0f MB > 126 MB L2)" % (n * 76 / 1e6),
                    "parallelism": f"replicas x{world}"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic,
-                     "bytes_per_node": bpn, "peak_kind": f"{peak_kind} copy bandwidth",
-                     "kernel": "k_phys_step<f32,BGK,force>"},
-        "variants": {"f16s": {"value": h_mlups, "unit": "MLUPS", "ms_per_step": h_ms / args.steps,
-                              "bytes_per_node": h_bpn, "achieved_gbs": h_ach,
-                              "frac": h_ach / peak, "speedup_vs_f32": h_mlups / mlups,
-                              "clocks": h_clocks}},
+        "roofline": {"bound": "hbm", "achieved": head["achieved_gbs"], "peak": peak, "unit": "GB/s",
+                     "frac": head["frac"], "traffic": traffic,
+                     "bytes_per_node": head["bytes_per_node"],
+                     "peak_kind": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)",
+                     "kernel": "k_phys_step (fused esoteric-pull stream+collide)"},
+        "variants": runs,
         "e2e": e2e,
         "gpu_launches": args.steps,
-        "clocks": clocks,
+        "clocks": head["clocks"],
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
@@ -335,6 +364,9 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end C-ABI run")
+    ap.add_argument("--variant", choices=["all", "f32", "f16s", "bf16s", "ref"], default="all",
+                    help="which device runs to do (profiling uses one)")
     args = ap.parse_args()
     world, rank, local = dist_setup(args.gpus)
     if args.impl == "reference":

@@ -109,6 +109,8 @@ int ensure_staging(Ctx* c, size_t bytes) {
 }
 
 void free_all(Ctx* c) {
+  for (auto& g : c->graph)
+    if (g) cudaGraphExecDestroy(g);
   void* ptrs[] = {c->fbuf[0], c->fbuf[1], c->pop,      c->mask,     c->flags, c->links,
                   c->rho,     c->u,       c->status,   c->partials, c->sums,  c->staging};
   for (void* p : ptrs)
@@ -346,20 +348,54 @@ int lbm_init_from_moments(lbm_ctx* c, const float* rho, const void* u, int u_fmt
   return LBM_OK;
 }
 
+// One step launch on stream s; flips the parity / current buffer.
+static cudaError_t launch_one(lbm_ctx* c, bool wm, cudaStream_t s) {
+  cudaError_t e;
+  if (c->d.mode == LBM_MODE_REFERENCE) {
+    e = lbm::ref_step(*c, c->fbuf[c->cur], c->fbuf[c->cur ^ 1], wm, s);
+    c->cur ^= 1;
+  } else {
+    e = lbm::phys_step(*c, c->parity, wm, s);
+    c->parity ^= 1;
+  }
+  return e;
+}
+
+// Captures kGraphSteps plain step launches, starting from the current parity,
+// on the context's own stream (a capture needs a non-legacy stream).  An even
+// count leaves the parity as it found it.
+static int build_graph(lbm_ctx* c, int slot) {
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(c->own_stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < Ctx::kGraphSteps && e == cudaSuccess; ++i) e = launch_one(c, false, c->own_stream);
+  cudaError_t e2 = cudaStreamEndCapture(c->own_stream, &g);
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return cuda_fail(c, e != cudaSuccess ? e : e2, "capture step graph");
+  }
+  e = cudaGraphInstantiate(&c->graph[slot], g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return cuda_fail(c, e, "instantiate step graph");
+  return LBM_OK;
+}
+
 int lbm_step(lbm_ctx* c, int nsteps) {
   if (int rc = check_ctx(c)) return rc;
   if (nsteps < 0) return fail(c, LBM_ERR_INVALID_ARG, "nsteps must be >= 0");
   if (!c->initialized) return fail(c, LBM_ERR_STATE, "lbm_step before lbm_init_*");
-  for (int i = 0; i < nsteps; ++i) {
-    const bool wm = (i == nsteps - 1);
-    cudaError_t e;
-    if (c->d.mode == LBM_MODE_REFERENCE) {
-      e = lbm::ref_step(*c, c->fbuf[c->cur], c->fbuf[c->cur ^ 1], wm, c->stream);
-      c->cur ^= 1;
-    } else {
-      e = lbm::phys_step(*c, c->parity, wm, c->stream);
-      c->parity ^= 1;
-    }
+  int left = nsteps;
+  // Whole graphs while more than kGraphSteps steps remain (the last launch
+  // of the call must write the moments, so it is never inside a graph).
+  while (left > Ctx::kGraphSteps) {
+    const int slot = c->d.mode == LBM_MODE_REFERENCE ? c->cur : c->parity;
+    if (!c->graph[slot])
+      if (int rc = build_graph(c, slot)) return rc;
+    CK(cudaGraphLaunch(c->graph[slot], c->stream), "graph launch");
+    left -= Ctx::kGraphSteps;
+  }
+  for (int i = 0; i < left; ++i) {
+    cudaError_t e = launch_one(c, i == left - 1, c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "step kernel launch");
   }
   c->iteration += (uint64_t)nsteps;

@@ -95,6 +95,10 @@ struct Ctx {
   int nblk_cons = 0;
   void* staging = nullptr;    // device staging for host format conversion
   size_t staging_bytes = 0;
+  // CUDA graphs of kGraphSteps step launches (no moment write), one per
+  // starting parity (reference mode: per current buffer), built on first use.
+  static constexpr int kGraphSteps = 16;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
   bool initialized = false;
   uint64_t iteration = 0;
   uint64_t dev_bytes = 0;
