@@ -133,6 +133,36 @@ namespace lbm {
 
 void set_thread_error(const char* msg) { g_thread_err = msg; }
 
+bool setup_physics(Ctx& c, const lbm_desc& d) {
+  auto& g = c.pp.g;
+  g.nx = d.nx; g.ny = d.ny; g.nz = d.nz;
+  g.n = (size_t)d.nx * d.ny * d.nz;
+  for (int a = 0; a < 3; ++a) g.per[a] = d.periodic[a];
+  g.px = g.per[0] ? g.nx : (int)round_up((size_t)g.nx + 1, 8);
+  g.gy = g.per[1] ? 0 : 1;
+  g.gz = g.per[2] ? 0 : 1;
+  g.py = g.ny + 2 * g.gy;
+  g.pz = g.nz + 2 * g.gz;
+  g.pxy = (uint32_t)((size_t)g.px * g.py);
+  g.slot_stride = round_up((size_t)g.px * g.py * g.pz, 64);
+  if (g.slot_stride >= (size_t(1) << 32)) return false;
+  auto& p = c.pp;
+  p.tau = d.tau;
+  p.omega = 1.0f / d.tau;
+  p.trt_magic = d.trt_magic;
+  p.smag_cs = d.smagorinsky_cs;
+  for (int a = 0; a < 3; ++a) p.accel[a] = d.body_accel[a];
+  p.any_moving_wall = 0;
+  for (int f = 0; f < 6; ++f)
+    for (int a = 0; a < 3; ++a) {
+      p.wall[f][a] = d.wall_velocity[f][a];
+      if (d.wall_velocity[f][a] != 0.f) p.any_moving_wall = 1;
+    }
+  return true;
+}
+
+int validate_desc(const lbm_desc* d) { return validate(d); }
+
 size_t elem_bytes(int precision) { return precision == LBM_PREC_F32 ? 4 : 2; }
 
 double bytes_per_node(const lbm_desc& d) {
@@ -203,34 +233,12 @@ int lbm_create(const lbm_desc* desc, lbm_ctx** out) {
     p.free_slip = desc->ref_free_slip;
     p.u_round = desc->ref_u_round;
   } else {
-    auto& g = c->pp.g;
-    g.nx = desc->nx; g.ny = desc->ny; g.nz = desc->nz; g.n = n;
-    for (int a = 0; a < 3; ++a) g.per[a] = desc->periodic[a];
-    g.px = g.per[0] ? g.nx : (int)round_up((size_t)g.nx + 1, 8);
-    g.gy = g.per[1] ? 0 : 1;
-    g.gz = g.per[2] ? 0 : 1;
-    g.py = g.ny + 2 * g.gy;
-    g.pz = g.nz + 2 * g.gz;
-    g.pxy = (uint32_t)((size_t)g.px * g.py);
-    g.slot_stride = round_up((size_t)g.px * g.py * g.pz, 64);
-    if (g.slot_stride >= (size_t(1) << 32))
+    if (!lbm::setup_physics(*c, *desc))
       return bail(fail(c, LBM_ERR_UNSUPPORTED, "padded grid exceeds 2^32 nodes per slot array"));
     const size_t eb = lbm::elem_bytes(desc->precision);
-    if ((rc = dev_alloc(c, reinterpret_cast<char**>(&c->pop), 19 * g.slot_stride * eb,
+    if ((rc = dev_alloc(c, reinterpret_cast<char**>(&c->pop), 19 * c->pp.g.slot_stride * eb,
                         "cudaMalloc(populations)")))
       return bail(rc);
-    auto& p = c->pp;
-    p.tau = desc->tau;
-    p.omega = 1.0f / desc->tau;
-    p.trt_magic = desc->trt_magic;
-    p.smag_cs = desc->smagorinsky_cs;
-    for (int a = 0; a < 3; ++a) p.accel[a] = desc->body_accel[a];
-    p.any_moving_wall = 0;
-    for (int f = 0; f < 6; ++f)
-      for (int a = 0; a < 3; ++a) {
-        p.wall[f][a] = desc->wall_velocity[f][a];
-        if (desc->wall_velocity[f][a] != 0.f) p.any_moving_wall = 1;
-      }
   }
   c->nblk_cons = lbm::cons_blocks(n);
   if ((rc = dev_alloc(c, &c->mask, n, "cudaMalloc(mask)")) ||

@@ -106,6 +106,11 @@ struct Ctx {
 };
 
 size_t elem_bytes(int precision);
+// Fills c.pp (padded geometry and physics parameters) from a physics-mode
+// descriptor; false if a slot array would exceed 2^32 elements.
+bool setup_physics(Ctx& c, const lbm_desc& d);
+int validate_desc(const lbm_desc* d);  // LBM_OK or an LBM_ERR_* (message set)
+void set_thread_error(const char* msg);
 double bytes_per_node(const lbm_desc& d);
 
 }  // namespace lbm

@@ -73,6 +73,22 @@ class Info(C.Structure):
     ]
 
 
+class BatchSchedule(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_uint32),
+        ("rows_per_block", C.c_int32), ("z_per_thread", C.c_int32), ("persistent", C.c_int32),
+        ("spin_limit_cycles", C.c_int64), ("test_missing_blocks", C.c_int32),
+    ]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_uint32), ("domains", C.c_int32), ("total_nodes", C.c_uint64),
+        ("tiles", C.c_uint32), ("grid", C.c_int32), ("iteration", C.c_uint64),
+        ("device_bytes", C.c_uint64), ("bytes_per_node", C.c_double),
+    ]
+
+
 # Every symbol include/lbm.h declares, with its ctypes signature.
 _P = C.c_void_p
 _SIGS = {
@@ -99,6 +115,22 @@ _SIGS = {
                                     C.c_float, C.c_float, _P, C.c_size_t]),
     "lbm_half_to_float": (C.c_int, [_P, _P, C.c_size_t]),
     "lbm_build_info": (C.c_char_p, []),
+    "lbm_batch_schedule_default": (C.c_int, [C.POINTER(BatchSchedule)]),
+    "lbm_batch_create": (C.c_int, [_P, C.c_int, C.POINTER(_P)]),
+    "lbm_batch_destroy": (C.c_int, [_P]),
+    "lbm_batch_set_stream": (C.c_int, [_P, _P]),
+    "lbm_batch_set_flags": (C.c_int, [_P, C.c_int, _P, C.c_size_t]),
+    "lbm_batch_init_equilibrium": (C.c_int, [_P, C.c_int, C.c_float, C.POINTER(C.c_float)]),
+    "lbm_batch_init_from_moments": (C.c_int, [_P, C.c_int, _P, _P, C.c_int]),
+    "lbm_batch_step": (C.c_int, [_P, C.c_int]),
+    "lbm_batch_sync": (C.c_int, [_P]),
+    "lbm_batch_read_moments": (C.c_int, [_P, C.c_int, _P, _P, C.c_int]),
+    "lbm_batch_read_populations": (C.c_int, [_P, C.c_int, _P, C.c_size_t]),
+    "lbm_batch_set_schedule": (C.c_int, [_P, C.POINTER(BatchSchedule)]),
+    "lbm_batch_get_schedule": (C.c_int, [_P, C.POINTER(BatchSchedule)]),
+    "lbm_batch_autotune": (C.c_int, [_P, C.c_int, C.POINTER(BatchSchedule)]),
+    "lbm_batch_get_info": (C.c_int, [_P, C.POINTER(BatchInfo)]),
+    "lbm_batch_last_error": (C.c_char_p, [_P]),
 }
 
 _lib = None
@@ -271,6 +303,96 @@ class Lattice:
         i = Info()
         i.struct_size = C.sizeof(Info)
         self._c(load().lbm_get_info(self._h, C.byref(i)))
+        return i
+
+
+class Batch:
+    """Many independent physics-mode domains advanced together (lbm_batch)."""
+
+    def __init__(self, descs):
+        lib = load()
+        self.descs = list(descs)
+        arr = (Desc * len(self.descs))(*self.descs)
+        h = _P()
+        rc = lib.lbm_batch_create(arr, len(self.descs), C.byref(h))
+        if rc != OK:
+            raise LbmError(rc, lib.lbm_last_error(None).decode())
+        self._h = h
+        self.shapes = [(d.nx, d.ny, d.nz) for d in self.descs]
+
+    def _c(self, rc: int) -> None:
+        if rc != OK:
+            raise LbmError(rc, load().lbm_batch_last_error(self._h).decode())
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            load().lbm_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def n(self, d: int) -> int:
+        nx, ny, nz = self.shapes[d]
+        return nx * ny * nz
+
+    def set_stream(self, stream_ptr) -> None:
+        self._c(load().lbm_batch_set_stream(self._h, stream_ptr))
+
+    def set_flags(self, d: int, mask: np.ndarray) -> None:
+        m = np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
+        self._c(load().lbm_batch_set_flags(self._h, d, _ptr(m), m.size))
+
+    def init_equilibrium(self, d: int = -1, rho0: float = 1.0, u0=(0.0, 0.0, 0.0)) -> None:
+        self._c(load().lbm_batch_init_equilibrium(self._h, d, rho0, (C.c_float * 3)(*u0)))
+
+    def init_from_moments(self, d: int, rho: np.ndarray, u: np.ndarray) -> None:
+        r = np.ascontiguousarray(rho, dtype=np.float32).reshape(-1)
+        uu = np.ascontiguousarray(u, dtype=np.float32)
+        self._c(load().lbm_batch_init_from_moments(self._h, d, _ptr(r), _ptr(uu), U_F32X3))
+
+    def step(self, nsteps: int = 1) -> None:
+        self._c(load().lbm_batch_step(self._h, nsteps))
+
+    def sync(self) -> None:
+        self._c(load().lbm_batch_sync(self._h))
+
+    def read_moments(self, d: int):
+        n = self.n(d)
+        rho = np.empty(n, np.float32)
+        u = np.empty((n, 3), np.float32)
+        self._c(load().lbm_batch_read_moments(self._h, d, _ptr(rho), _ptr(u), U_F32X3))
+        return rho, u
+
+    def read_populations(self, d: int) -> np.ndarray:
+        f = np.empty((19, self.n(d)), np.float32)
+        self._c(load().lbm_batch_read_populations(self._h, d, _ptr(f), f.size))
+        return f
+
+    def schedule(self) -> BatchSchedule:
+        s = BatchSchedule()
+        self._c(load().lbm_batch_get_schedule(self._h, C.byref(s)))
+        return s
+
+    def set_schedule(self, **kw) -> None:
+        s = self.schedule()
+        for k, v in kw.items():
+            setattr(s, k, v)
+        self._c(load().lbm_batch_set_schedule(self._h, C.byref(s)))
+
+    def autotune(self, trial_steps: int = 10) -> BatchSchedule:
+        s = BatchSchedule()
+        s.struct_size = C.sizeof(BatchSchedule)
+        self._c(load().lbm_batch_autotune(self._h, trial_steps, C.byref(s)))
+        return s
+
+    def info(self) -> BatchInfo:
+        i = BatchInfo()
+        i.struct_size = C.sizeof(BatchInfo)
+        self._c(load().lbm_batch_get_info(self._h, C.byref(i)))
         return i
 
 

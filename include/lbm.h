@@ -202,6 +202,62 @@ LBM_API const char* lbm_last_error(lbm_ctx* ctx);
 LBM_API int lbm_conservation_noalloc(const float* d_rho, const float* d_u, size_t n,
                                      double out[4], void* stream);
 
+/* ---- batched ensemble --------------------------------------------------- */
+/* Hundreds of independent physics-mode domains of uneven size advanced
+ * together: one launch per step over a tile work-list (captured in a CUDA
+ * graph), or one persistent cooperative launch per lbm_batch_step call.  The
+ * reference runs one domain at a time (src/main.cpp:1554-1591); a batch is
+ * equivalent to lbm_step on each domain alone, bit for bit. */
+typedef struct lbm_batch lbm_batch;
+
+typedef struct lbm_batch_schedule {
+    uint32_t struct_size;
+    int32_t  rows_per_block;      /* 1, 2, 4, 8: a block is 32 x rows threads */
+    int32_t  z_per_thread;        /* 1..8 nodes along z per thread            */
+    int32_t  persistent;          /* 1 = one cooperative launch per call      */
+    int64_t  spin_limit_cycles;   /* bound of a grid-barrier wait (persistent)*/
+    int32_t  test_missing_blocks; /* testing only: barrier waits for this many
+                                     blocks that never arrive -> TIMEOUT      */
+} lbm_batch_schedule;
+
+typedef struct lbm_batch_info {
+    uint32_t struct_size;
+    int32_t  domains;
+    uint64_t total_nodes;
+    uint32_t tiles;
+    int32_t  grid;                /* persistent grid size (0 in graph mode)   */
+    uint64_t iteration;
+    uint64_t device_bytes;
+    double   bytes_per_node;
+} lbm_batch_info;
+
+LBM_API int lbm_batch_schedule_default(lbm_batch_schedule* s);
+/* All descriptors: physics mode, one precision and collision for all, no
+ * Smagorinsky term, no body force.  Domains start all-fluid. */
+LBM_API int lbm_batch_create(const lbm_desc* descs, int n, lbm_batch** out);
+LBM_API int lbm_batch_destroy(lbm_batch* b);
+LBM_API int lbm_batch_set_stream(lbm_batch* b, void* stream);
+LBM_API int lbm_batch_set_flags(lbm_batch* b, int domain, const uint8_t* mask, size_t n);
+/* domain = -1 initialises every domain. */
+LBM_API int lbm_batch_init_equilibrium(lbm_batch* b, int domain, float rho0, const float u0[3]);
+LBM_API int lbm_batch_init_from_moments(lbm_batch* b, int domain, const float* rho,
+                                        const void* u, int u_fmt);
+LBM_API int lbm_batch_step(lbm_batch* b, int nsteps);
+/* LBM_ERR_NONFINITE as lbm_sync; LBM_ERR_TIMEOUT if a persistent launch's
+ * grid barrier gave up (the domains then need a new init). */
+LBM_API int lbm_batch_sync(lbm_batch* b);
+LBM_API int lbm_batch_read_moments(lbm_batch* b, int domain, float* rho, void* u, int u_fmt);
+LBM_API int lbm_batch_read_populations(lbm_batch* b, int domain, float* f, size_t n);
+LBM_API int lbm_batch_set_schedule(lbm_batch* b, const lbm_batch_schedule* s);
+LBM_API int lbm_batch_get_schedule(lbm_batch* b, lbm_batch_schedule* s);
+/* Times every schedule (rows 2/4/8 x z 1/2/4 x graph/persistent) for
+ * trial_steps steps, keeps the fastest and restores the populations.  Results
+ * are cached per (precision, collision, size class) for the process and, if
+ * $LBM_AUTOTUNE_CACHE names a file, across processes. */
+LBM_API int lbm_batch_autotune(lbm_batch* b, int trial_steps, lbm_batch_schedule* best);
+LBM_API int lbm_batch_get_info(lbm_batch* b, lbm_batch_info* info);
+LBM_API const char* lbm_batch_last_error(lbm_batch* b);
+
 /* ---- host-side helpers (no GPU needed) --------------------------------- */
 
 /* D3Q19 tables in the reference's direction order
