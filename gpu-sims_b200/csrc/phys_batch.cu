@@ -61,8 +61,12 @@ __device__ __forceinline__ void batch_tile(const BatchDomain& D, uint32_t local,
   }
 }
 
+#ifndef LBM_BATCH_MINB
+#define LBM_BATCH_MINB 3
+#endif
+
 template <int PREC, int COLL, bool WM, int P>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, LBM_BATCH_MINB)
     k_batch_step(const BatchDomain* __restrict__ dp, int ndom, int nzt, unsigned* status) {
   __shared__ BatchDomain sD;
   __shared__ uint32_t s_local;
@@ -106,7 +110,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned expected, l
 }
 
 template <int PREC, int COLL>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, LBM_BATCH_MINB)
     k_batch_persistent(const BatchDomain* __restrict__ dp, int ndom, uint32_t ntiles, int nzt,
                        int nsteps, int P0, unsigned* bar, unsigned expected, long long spin,
                        unsigned* status) {

@@ -1,0 +1,127 @@
+"""Workload definitions of the BASELINE configurations and the ensemble run.
+
+    python -m lbm.configs ensemble [--steps 2000] [--domains 256]
+
+(run from gpu-sims_b200/, or with it on sys.path) prints one JSON line: the
+aggregate MLUPS of the 256-cavity ensemble in fp16 and fp32 storage and the
+per-domain fp16-vs-fp32 velocity error.  All inputs are synthetic and seeded;
+device time is measured with CUDA events on the library's stream.  The FP64
+comparisons of the cavity, Taylor-Green and channel workloads are GPU tests
+(tests/test_configs_gpu.py).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import sys
+import time
+
+import numpy as np
+
+import lbm
+
+EDGES = (32, 48, 64, 80, 96)
+LID = 0.05
+
+
+def _timer():
+    import torch
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+
+    def run(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3
+
+    return stream, run
+
+
+def ensemble_descs(n=256, seed=2024, precision=lbm.PREC_F16S, collision=lbm.COLL_TRT):
+    """n lid-driven cavities: edge uniform from {32,48,64,80,96}, Re uniform in
+    [100, 1000], tau = 0.5 + 3 nu with nu = U L / Re, lid U = 0.05 along +x on
+    the z = max face, half-way bounce-back on the other five walls.  TRT by
+    default: with BGK the 32- and 48-node cavities at tau below about 0.508
+    (38 of the 256 for seed 2024) diverge in fp32 and fp16 alike."""
+    rng = np.random.default_rng(seed)
+    edges = rng.choice(EDGES, size=n)
+    res = rng.uniform(100.0, 1000.0, size=n)
+    descs = []
+    for L, re in zip(edges, res):
+        wall = np.zeros((6, 3))
+        wall[lbm.FACE_ZP] = (LID, 0.0, 0.0)
+        tau = 0.5 + 3.0 * LID * float(L) / float(re)
+        descs.append(lbm.default_desc(nx=int(L), ny=int(L), nz=int(L), mode=lbm.MODE_PHYSICS,
+                                      precision=precision, collision=collision, tau=tau,
+                                      wall_velocity=wall))
+    return descs, edges, res
+
+
+def run_ensemble(steps=2000, n=256, seed=2024, autotune=True, compare=True):
+    stream, timed = _timer()
+    out = {"config": "ensemble", "domains": n, "steps": steps}
+    fields = {}
+    for name, prec in (("f16s", lbm.PREC_F16S), ("f32", lbm.PREC_F32)):
+        if name == "f32" and not compare:
+            break
+        descs, edges, res = ensemble_descs(n, seed, prec)
+        b = lbm.Batch(descs)
+        b.set_stream(stream.cuda_stream)
+        b.init_equilibrium(-1, 1.0, (0.0, 0.0, 0.0))
+        sched = b.autotune(10) if autotune else b.schedule()
+        info = b.info()
+        b.init_equilibrium(-1, 1.0, (0.0, 0.0, 0.0))
+        secs = timed(lambda: b.step(steps))
+        b.sync()
+        mlups = info.total_nodes * steps / secs / 1e6
+        out[name] = {"mlups": mlups, "seconds": secs, "total_nodes": info.total_nodes,
+                     "bytes_per_node": info.bytes_per_node,
+                     "achieved_gbs": mlups * 1e6 * info.bytes_per_node / 1e9,
+                     "schedule": {"rows_per_block": sched.rows_per_block,
+                                  "z_per_thread": sched.z_per_thread,
+                                  "persistent": sched.persistent},
+                     "device_bytes": info.device_bytes}
+        fields[name] = [b.read_moments(i)[1] for i in range(n)]
+        b.close()
+        out["edges_histogram"] = {int(e): int((edges == e).sum()) for e in EDGES}
+    if compare:
+        errs = np.array([np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+                         for a, b in zip(fields["f16s"], fields["f32"])])
+        out["f16s_vs_f32_rel_l2_velocity"] = {"max": float(errs.max()), "median": float(np.median(errs)),
+                                              "mean": float(errs.mean())}
+        out["speedup_f16s_vs_f32"] = out["f16s"]["mlups"] / out["f32"]["mlups"]
+    return out
+
+
+def tgv_init(N, u0=0.05):
+    """Taylor-Green vortex on an N^3 periodic box (wavelength N): velocity and
+    the density carrying the analytic pressure rho = 1 + 3 p'."""
+    k = 2.0 * math.pi / N
+    x = np.arange(N)
+    Z, Y, X = np.meshgrid(x, x, x, indexing="ij")
+    ux = u0 * np.sin(k * X) * np.cos(k * Y) * np.cos(k * Z)
+    uy = -u0 * np.cos(k * X) * np.sin(k * Y) * np.cos(k * Z)
+    p = u0 ** 2 / 16.0 * (np.cos(2 * k * X) + np.cos(2 * k * Y)) * (np.cos(2 * k * Z) + 2.0)
+    rho = 1.0 + 3.0 * p
+    u = np.stack([ux, uy, np.zeros_like(ux)]).reshape(3, -1)
+    return rho.reshape(-1), u
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("config", choices=["ensemble"])
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--domains", type=int, default=256)
+    a = ap.parse_args(argv)
+    r = run_ensemble(steps=a.steps or 2000, n=a.domains)
+    print(json.dumps(r), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -29,6 +29,8 @@
 // operation rounds on its own, in source order.
 #include <omp.h>
 
+#include "ext_step.h"
+
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -212,95 +214,6 @@ void ref_moments(const RefP& p, const float* f, float* rho, float* u) {
   }
 }
 
-// ---------------------------------------------------------------------------
-// ExtStep: textbook physics on plain populations.
-// ---------------------------------------------------------------------------
-struct ExtP {
-  int nx, ny, nz;
-  int periodic[3];
-  double tau;
-  int collision;  // 0 BGK, 1 TRT
-  double trt_magic;
-  double smag_cs;
-  double accel[3];
-  double wall[6][3];
-};
-
-// Population arriving at n in direction i: pulled from n - c_i; if that
-// node is solid or outside a non-periodic face, the half-way bounce-back
-// value f*_opp(i)(n) plus the moving-wall term 6 w_i (c_i . u_w), rho_w = 1.
-// The wall velocity is the one of the face the link leaves through (z, then
-// y, then x); links into interior solids see a resting wall.
-template <class T>
-T incoming(const ExtP& p, const uint8_t* mask, const T* f, int x, int y, int z, int i, size_t N) {
-  int xs = x - C[i][0], ys = y - C[i][1], zs = z - C[i][2];
-  int face = -1;
-  bool out = false;
-  if (zs < 0 || zs >= p.nz) { if (p.periodic[2]) zs = (zs + p.nz) % p.nz; else { out = true; face = zs < 0 ? 4 : 5; } }
-  if (ys < 0 || ys >= p.ny) { if (p.periodic[1]) ys = (ys + p.ny) % p.ny; else { out = true; if (face < 0) face = ys < 0 ? 2 : 3; } }
-  if (xs < 0 || xs >= p.nx) { if (p.periodic[0]) xs = (xs + p.nx) % p.nx; else { out = true; if (face < 0) face = xs < 0 ? 0 : 1; } }
-  const size_t n = idx(p.nx, p.ny, x, y, z);
-  if (!out && mask[idx(p.nx, p.ny, xs, ys, zs)] != 1) return f[i * N + idx(p.nx, p.ny, xs, ys, zs)];
-  T v = f[OPP[i] * N + n];
-  if (face >= 0) {
-    const double cu = C[i][0] * p.wall[face][0] + C[i][1] * p.wall[face][1] + C[i][2] * p.wall[face][2];
-    v += T(6.0 * weight<double>(i) * cu);
-  }
-  return v;
-}
-
-template <class T>
-void ext_collide_node(const ExtP& p, T* v, T& rho_o, T& ux_o, T& uy_o, T& uz_o) {
-  T rho = 0, jx = 0, jy = 0, jz = 0;
-  for (int i = 0; i < 19; ++i) {
-    rho += v[i];
-    jx += v[i] * T(C[i][0]);
-    jy += v[i] * T(C[i][1]);
-    jz += v[i] * T(C[i][2]);
-  }
-  const T ax = T(p.accel[0]), ay = T(p.accel[1]), az = T(p.accel[2]);
-  const T ux = jx / rho + ax / T(2), uy = jy / rho + ay / T(2), uz = jz / rho + az / T(2);
-  rho_o = rho; ux_o = ux; uy_o = uy; uz_o = uz;
-  const T Fx = rho * ax, Fy = rho * ay, Fz = rho * az;
-  T feq[19];
-  for (int i = 0; i < 19; ++i) feq[i] = feq_i<T>(i, rho, ux, uy, uz);
-  T tau = T(p.tau);
-  if (p.smag_cs > 0) {
-    T P[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    for (int i = 0; i < 19; ++i)
-      for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 3; ++b) P[a][b] += T(C[i][a] * C[i][b]) * (v[i] - feq[i]);
-    T q = 0;
-    for (int a = 0; a < 3; ++a)
-      for (int b = 0; b < 3; ++b) q += P[a][b] * P[a][b];
-    const T cs2 = T(p.smag_cs * p.smag_cs);
-    tau = (tau + std::sqrt(tau * tau + T(18) * std::sqrt(T(2)) * cs2 * std::sqrt(q) / rho)) / T(2);
-  }
-  const T om = T(1) / tau;
-  T src[19];
-  for (int i = 0; i < 19; ++i) {
-    const T cu = T(C[i][0]) * ux + T(C[i][1]) * uy + T(C[i][2]) * uz;
-    const T cF = T(C[i][0]) * Fx + T(C[i][1]) * Fy + T(C[i][2]) * Fz;
-    const T uF = ux * Fx + uy * Fy + uz * Fz;
-    src[i] = weight<T>(i) * (T(3) * (cF - uF) + T(9) * cu * cF);  // Guo term without prefactor
-  }
-  if (p.collision == 0) {
-    for (int i = 0; i < 19; ++i) v[i] = v[i] + om * (feq[i] - v[i]) + (T(1) - om / T(2)) * src[i];
-  } else {
-    const T om_m = T(1) / (T(p.trt_magic) / (tau - T(0.5)) + T(0.5));
-    T out[19];
-    for (int i = 0; i < 19; ++i) {
-      const int j = OPP[i];
-      const T fp = (v[i] + v[j]) / T(2), fm = (v[i] - v[j]) / T(2);
-      const T ep = (feq[i] + feq[j]) / T(2), em = (feq[i] - feq[j]) / T(2);
-      const T sp = (src[i] + src[j]) / T(2), sm = (src[i] - src[j]) / T(2);
-      out[i] = v[i] - om * (fp - ep) - om_m * (fm - em) + (T(1) - om / T(2)) * sp +
-               (T(1) - om_m / T(2)) * sm;
-    }
-    for (int i = 0; i < 19; ++i) v[i] = out[i];
-  }
-}
-
 static RefP make_ref(const int* ip, const float* fp) {
   RefP p;
   p.nx = ip[0]; p.ny = ip[1]; p.nz = ip[2];
@@ -311,20 +224,11 @@ static RefP make_ref(const int* ip, const float* fp) {
   return p;
 }
 
-// --- ExtStep -----------------------------------------------------------------
-// ip: nx ny nz px py pz collision; dp: tau trt_magic smag_cs accel[3] wall[18]
-
-static ExtP make_ext(const int* ip, const double* dp) {
-  ExtP p;
-  p.nx = ip[0]; p.ny = ip[1]; p.nz = ip[2];
-  p.periodic[0] = ip[3]; p.periodic[1] = ip[4]; p.periodic[2] = ip[5];
-  p.collision = ip[6];
-  p.tau = dp[0]; p.trt_magic = dp[1]; p.smag_cs = dp[2];
-  for (int a = 0; a < 3; ++a) p.accel[a] = dp[3 + a];
-  for (int f = 0; f < 6; ++f)
-    for (int a = 0; a < 3; ++a) p.wall[f][a] = dp[6 + 3 * f + a];
-  return p;
-}
+// ---------------------------------------------------------------------------
+// ExtStep drivers (node update in ext_step.h, shared with the FP64 GPU copy).
+// ---------------------------------------------------------------------------
+using ox::ExtP;
+using ox::make_ext;
 
 template <class T>
 static void ext_init_t(const int* ip, const double* dp, const uint8_t* mask, const T* rho,
@@ -335,7 +239,7 @@ static void ext_init_t(const int* ip, const double* dp, const uint8_t* mask, con
   for (long long n = 0; n < (long long)N; ++n) {
     const bool solid = mask[n] == 1;
     for (int i = 0; i < 19; ++i)
-      f[i * N + n] = solid ? T(0) : feq_i<T>(i, rho[n], u[n], u[N + n], u[2 * N + n]);
+      f[i * N + n] = solid ? T(0) : ox::feq_i<T>(i, rho[n], u[n], u[N + n], u[2 * N + n]);
   }
 }
 
@@ -358,9 +262,9 @@ static void ext_step_t(const int* ip, const double* dp, const uint8_t* mask, T* 
             continue;
           }
           T v[19];
-          for (int i = 0; i < 19; ++i) v[i] = incoming<T>(p, mask, f, x, y, z, i, N);
+          for (int i = 0; i < 19; ++i) v[i] = ox::incoming<T>(p, mask, f, x, y, z, i, N);
           T r, ux, uy, uz;
-          ext_collide_node<T>(p, v, r, ux, uy, uz);
+          ox::ext_collide_node<T>(p, v, r, ux, uy, uz);
           for (int i = 0; i < 19; ++i) g[i * N + n] = v[i];
           if (last && rho_o) { rho_o[n] = r; u_o[n] = ux; u_o[N + n] = uy; u_o[2 * N + n] = uz; }
         }

@@ -172,3 +172,69 @@ class ExtState:
     def step(self, n=1):
         fn = lib().oracle_ext_step_f64 if self.dtype == np.float64 else lib().oracle_ext_step_f32
         fn(_p(self.ip), _p(self.dp), _p(self.mask), _p(self.f), n, _p(self.rho), _p(self.u))
+
+
+LIB_GPU = HERE / "liboracle_gpu.so"
+_lib_gpu = None
+
+
+def lib_gpu() -> C.CDLL:
+    global _lib_gpu
+    if _lib_gpu is None:
+        if not LIB_GPU.exists():
+            build()
+        L = C.CDLL(str(LIB_GPU))
+        L.oracle_gpu_ext_init_f64.restype = C.c_int
+        L.oracle_gpu_ext_init_f64.argtypes = [_P] * 6
+        L.oracle_gpu_ext_step_f64.restype = C.c_int
+        L.oracle_gpu_ext_step_f64.argtypes = [_P, _P, _P, _P, _P, C.c_int, _P, _P]
+        _lib_gpu = L
+    return _lib_gpu
+
+
+class ExtStateGPU:
+    """FP64 ExtStep on the current CUDA device (same node update as ExtState,
+    bit for bit); device memory through torch.  For full-size FP64 runs."""
+
+    def __init__(self, shape, periodic=(0, 0, 0), tau=0.6, collision=0, trt_magic=3.0 / 16.0,
+                 smag_cs=0.0, accel=(0.0, 0.0, 0.0), wall=None, mask=None):
+        import torch
+        self.torch = torch
+        self.shape = tuple(shape)
+        nx, ny, nz = self.shape
+        self.n = nx * ny * nz
+        self.ip = np.array([nx, ny, nz, *periodic, collision], np.int32)
+        w = np.zeros((6, 3)) if wall is None else np.asarray(wall, np.float64).reshape(6, 3)
+        self.dp = np.ascontiguousarray(np.concatenate([[tau, trt_magic, smag_cs],
+                                                       np.asarray(accel, np.float64), w.reshape(-1)]))
+        m = np.zeros(self.n, np.uint8) if mask is None else np.ascontiguousarray(mask, np.uint8).reshape(-1)
+        dev = torch.device("cuda")
+        self.mask = torch.from_numpy(m).to(dev)
+        self.f = torch.zeros(19 * self.n, dtype=torch.float64, device=dev)
+        self.tmp = torch.zeros_like(self.f)
+        self.rho = torch.zeros(self.n, dtype=torch.float64, device=dev)
+        self.u = torch.zeros(3 * self.n, dtype=torch.float64, device=dev)
+
+    def init(self, rho, u):
+        t = self.torch
+        r = t.from_numpy(np.ascontiguousarray(np.broadcast_to(rho, (self.n,)), np.float64)).cuda()
+        uu = t.from_numpy(np.ascontiguousarray(np.asarray(u, np.float64).reshape(3, -1) * np.ones((3, self.n)))).cuda()
+        t.cuda.synchronize()
+        rc = lib_gpu().oracle_gpu_ext_init_f64(self.ip.ctypes.data, self.dp.ctypes.data, self.mask.data_ptr(),
+                                               r.data_ptr(), uu.data_ptr(), self.f.data_ptr())
+        assert rc == 0, rc
+        self.rho.copy_(r)
+        self.u.copy_(uu.reshape(-1))
+        solid = self.mask == 1
+        self.rho[solid] = 0
+        self.u.view(3, -1)[:, solid] = 0
+
+    def step(self, n=1):
+        self.torch.cuda.synchronize()
+        rc = lib_gpu().oracle_gpu_ext_step_f64(self.ip.ctypes.data, self.dp.ctypes.data, self.mask.data_ptr(),
+                                               self.f.data_ptr(), self.tmp.data_ptr(), n,
+                                               self.rho.data_ptr(), self.u.data_ptr())
+        assert rc == 0, rc
+
+    def moments(self):
+        return self.rho.cpu().numpy(), self.u.view(3, -1).cpu().numpy()
