@@ -48,6 +48,7 @@ __host__ __device__ constexpr int pair_b(int p) { return opp(pair_a(p)); }
 // Node-classification bits (flag byte per node).
 constexpr uint8_t FLAG_SOLID = 1u;     // mask value 1
 constexpr uint8_t FLAG_BOUNDARY = 2u;  // fluid node with a blocked link
+constexpr uint8_t FLAG_SOLID_LINK = 4u;  // ... of which one ends at a solid node of the grid
 
 // ---------------------------------------------------------------------------
 // Reference-literal arithmetic.  Each operation is a separately rounded fp32

@@ -276,6 +276,14 @@ __device__ __forceinline__ void step_row(const PhysParams& p, void* __restrict__
   const uint32_t ln = lin32(G, xc, y, z);
   const Wrap w = wrap_terms(G, xc, y, z);
 
+  // Faces of non-periodic axes at this node: links across them are half-way
+  // bounce-back links known from the coordinates, so their slots are read in
+  // the first batch of loads (the y and z parts are uniform over the warp).
+  const bool xlo = !G.per[0] && xc == 0, xhi = !G.per[0] && xc == G.nx - 1;
+  const bool ylo = !G.per[1] && y == 0, yhi = !G.per[1] && y == G.ny - 1;
+  const bool zlo = !G.per[2] && z == 0, zhi = !G.per[2] && z == G.nz - 1;
+  const bool moving = p.any_moving_wall;
+
   const uint8_t fl = valid ? flags[nid] : FLAG_SOLID;
   float g[Q];
   g[0] = S::raw_ld(pop, ln);
@@ -286,35 +294,57 @@ __device__ __forceinline__ void step_row(const PhysParams& p, void* __restrict__
     const T* s0 = pop + (size_t)(1 + 2 * pi) * SS;
     const T* sP = P ? s0 + SS : s0;
     const T* sQ = P ? s0 : s0 + SS;
-    g[a] = S::raw_ld(sQ, ln);
+    // n + d (forward) or n - d (backward) beyond a wall face
+    const bool fyz = (DY > 0 && yhi) || (DY < 0 && ylo) || (DZ > 0 && zhi) || (DZ < 0 && zlo);
+    const bool fwd_wall = fyz || (DX > 0 && xhi);
+    const bool bwd_wall =
+        (DX > 0 && xlo) || (DY > 0 && ylo) || (DY < 0 && yhi) || (DZ > 0 && zlo) || (DZ < 0 && zhi);
+    // f_a from X = S[1-P](n), or f*_b(n) from S[P](n) across a wall
+    g[a] = S::raw_ld(bwd_wall ? sP : sQ, ln);
+    // f_b from Y = S[P](n+d), or f*_a(n) from S[1-P](n+d) across a wall
     if (DX == 0) {
-      g[b] = S::raw_ld(sP, ln + offs<0, DY, DZ>(G, w));
+      g[b] = S::raw_ld(fwd_wall ? sQ : sP, ln + offs<0, DY, DZ>(G, w));
     } else {
-      const float own = S::raw_ld(sP, ln + offs<0, DY, DZ>(G, w));
+      const float own = S::raw_ld(fyz ? sQ : sP, ln + offs<0, DY, DZ>(G, w));
       float nb = __shfl_down_sync(FULL, own, 1);
-      if (edge) nb = S::raw_ld(sP, ln + offs<1, DY, DZ>(G, w));
+      if (edge) nb = S::raw_ld(fwd_wall ? sQ : sP, ln + offs<1, DY, DZ>(G, w));
       g[b] = nb;
     }
   });
-
-  const bool fluid = valid && !(fl & FLAG_SOLID);
-  if (fluid && (fl & FLAG_BOUNDARY)) {
-    const uint32_t L = links[nid];
-    const bool moving = p.any_moving_wall;
+  // Moving-wall momentum terms, in a pass of their own: inside the load loop
+  // even a predicated-off add would wait for its load and serialise them.
+  if (moving) {
     static_for<0, 9>([&](auto PI) {
       constexpr int pi = decltype(PI)::value;
       constexpr int a = pair_a(pi), b = pair_b(pi);
+      constexpr int DX = cx(a), DY = cy(a), DZ = cz(a);
+      const bool fwd_wall = (DX > 0 && xhi) || (DY > 0 && yhi) || (DY < 0 && ylo) || (DZ > 0 && zhi) ||
+                            (DZ < 0 && zlo);
+      const bool bwd_wall =
+          (DX > 0 && xlo) || (DY > 0 && ylo) || (DY < 0 && yhi) || (DZ > 0 && zlo) || (DZ < 0 && zhi);
+      if (bwd_wall) g[a] = fmaf(S::SC, wall_term<a>(p, x, y, z), g[a]);
+      if (fwd_wall) g[b] = fmaf(S::SC, wall_term<b>(p, x, y, z), g[b]);
+    });
+  }
+
+  const bool fluid = valid && !(fl & FLAG_SOLID);
+  // Links into interior solid nodes (resting walls) need the classification
+  // word: a second, rare round trip.
+  if (fluid && (fl & FLAG_SOLID_LINK)) {
+    const uint32_t L = links[nid];
+    static_for<0, 9>([&](auto PI) {
+      constexpr int pi = decltype(PI)::value;
+      constexpr int a = pair_a(pi), b = pair_b(pi);
+      constexpr int DX = cx(a), DY = cy(a), DZ = cz(a);
       const T* s0 = pop + (size_t)(1 + 2 * pi) * SS;
       const T* sP = P ? s0 + SS : s0;
       const T* sQ = P ? s0 : s0 + SS;
-      if ((L >> b) & 1u) {  // n - d is a wall: f_a(n) = f*_b(n) from S[P](n)
-        g[a] = S::raw_ld(sP, ln);
-        if (moving) g[a] = fmaf(S::SC, wall_term<a>(p, x, y, z), g[a]);
-      }
-      if ((L >> a) & 1u) {  // n + d is a wall: f_b(n) = f*_a(n) from S[1-P](n+d)
-        g[b] = S::raw_ld(sQ, ln + offs<cx(a), cy(a), cz(a)>(G, w));
-        if (moving) g[b] = fmaf(S::SC, wall_term<b>(p, x, y, z), g[b]);
-      }
+      const bool fwd_wall = (DX > 0 && xhi) || (DY > 0 && yhi) || (DY < 0 && ylo) || (DZ > 0 && zhi) ||
+                            (DZ < 0 && zlo);
+      const bool bwd_wall =
+          (DX > 0 && xlo) || (DY > 0 && ylo) || (DY < 0 && yhi) || (DZ > 0 && zlo) || (DZ < 0 && zhi);
+      if (((L >> b) & 1u) && !bwd_wall) g[a] = S::raw_ld(sP, ln);
+      if (((L >> a) & 1u) && !fwd_wall) g[b] = S::raw_ld(sQ, ln + offs<DX, DY, DZ>(G, w));
     });
   }
 

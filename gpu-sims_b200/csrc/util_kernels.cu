@@ -11,7 +11,9 @@ namespace {
 // x + c_i is solid, where a neighbour outside the box counts as solid on a
 // non-periodic axis (mask_at, shaders/apply_boundaries.comp.glsl:52-55) and
 // wraps on a periodic one.  FLAG_BOUNDARY marks fluid nodes with any link
-// bit, the only nodes whose step needs the word.
+// bit (the reference-mode step reads the word there); FLAG_SOLID_LINK those
+// with a link to a solid node of the grid (the physics-mode step derives
+// wall links from the coordinates and reads the word only there).
 __global__ void __launch_bounds__(256)
     k_classify(int nx, int ny, int nz, int px, int py, int pz, const uint8_t* __restrict__ mask,
                uint8_t* __restrict__ flags, uint32_t* __restrict__ links) {
@@ -22,6 +24,7 @@ __global__ void __launch_bounds__(256)
   const size_t nid = (size_t)x + (size_t)nx * ((size_t)y + (size_t)ny * (size_t)z);
   const bool solid = mask[nid] == 1;
   uint32_t L = solid ? 1u : 0u;
+  bool to_solid = false;
   static_for<1, Q>([&](auto I) {
     constexpr int i = decltype(I)::value;
     int xn = x + cx(i), yn = y + cy(i), zn = z + cz(i);
@@ -30,11 +33,15 @@ __global__ void __launch_bounds__(256)
     if (yn < 0 || yn >= ny) { if (py) yn = (yn + ny) % ny; else oob = true; }
     if (zn < 0 || zn >= nz) { if (pz) zn = (zn + nz) % nz; else oob = true; }
     bool s = oob;
-    if (!oob) s = mask[(size_t)xn + (size_t)nx * ((size_t)yn + (size_t)ny * (size_t)zn)] == 1;
+    if (!oob) {
+      s = mask[(size_t)xn + (size_t)nx * ((size_t)yn + (size_t)ny * (size_t)zn)] == 1;
+      to_solid = to_solid || s;
+    }
     if (s) L |= 1u << i;
   });
   links[nid] = L;
-  flags[nid] = solid ? FLAG_SOLID : ((L >> 1) ? FLAG_BOUNDARY : 0);
+  flags[nid] = solid ? FLAG_SOLID
+                     : (uint8_t)(((L >> 1) ? FLAG_BOUNDARY : 0) | (to_solid ? FLAG_SOLID_LINK : 0));
 }
 
 }  // namespace
