@@ -55,6 +55,7 @@ def build(force: bool = False, verbose: bool = False, out: Path | None = None,
     OUT = out or OUT
     extra = [f"-D{d}" for d in (defines or [])]
     BUILD.mkdir(parents=True, exist_ok=True)
+    OUT.parent.mkdir(parents=True, exist_ok=True)
     cc = nvcc()
     objs = []
     for src in sources():

@@ -114,7 +114,8 @@ int build_tiles(lbm_batch* b) {
     D.links = v.links;
     D.rho = v.rho;
     D.u = v.u;
-    D.tiles_x = (v.d.nx + 31) / 32;
+    D.pairs = lbm::step_pairs_host(v.d.nx) ? 1u : 0u;
+    D.tiles_x = D.pairs ? (v.d.nx + 63) / 64 : (v.d.nx + 31) / 32;
     D.tiles_y = (v.d.ny + R - 1) / R;
     D.tile_begin = (uint32_t)t;
     t += (uint64_t)D.tiles_x * D.tiles_y * ((v.d.nz + Z - 1) / Z);

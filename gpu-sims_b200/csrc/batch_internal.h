@@ -19,9 +19,9 @@ struct BatchDomain {
   const uint32_t* links;
   float* rho;
   float* u;
-  int tiles_x, tiles_y;   // ceil(nx / 32), ceil(ny / rows)
+  int tiles_x, tiles_y;   // ceil(nx / (32 or 64)), ceil(ny / rows)
   uint32_t tile_begin;    // index of this domain's first tile
-  uint32_t pad;
+  uint32_t pairs;         // 1: two nodes per thread (tiles 64 wide)
 };
 static_assert(sizeof(BatchDomain) % 4 == 0, "copied as 32-bit words");
 

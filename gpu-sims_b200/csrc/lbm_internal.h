@@ -49,6 +49,10 @@ struct PhysParams {
 
 struct Ctx;
 
+// Whether the physics step runs two nodes per thread for this row length
+// (the rule lives with the step, phys_step.cuh).
+bool step_pairs_host(int nx);
+
 // reference-mode kernels (ref_kernels.cu)
 cudaError_t ref_init(const Ctx& c, const float* rho, const float* u3, float rho0,
                      const float* u0, cudaStream_t s);

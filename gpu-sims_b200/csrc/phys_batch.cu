@@ -2,12 +2,14 @@
 // launch per step (graph mode) or one cooperative launch for many steps
 // (persistent mode).
 //
-// Work list.  Every domain is cut into tiles of 32 x R x Z nodes (R rows per
-// block, Z z-planes per thread, chosen by the schedule/autotuner); tiles are
+// Work list.  Every domain is cut into tiles of 32 (64 when a thread takes two
+// nodes) x R x Z nodes (R rows per block, Z z-planes per thread, chosen by the
+// schedule/autotuner); tiles are
 // numbered domain after domain and a block finds its domain by binary search
 // over the first-tile table, then copies that domain's parameters into shared
-// memory.  The node update is the single-domain step_row (phys_step.cuh), so a
-// domain advanced in a batch is bit-identical to the same domain advanced alone.
+// memory.  The node update is the single-domain step_row / step_row2
+// (phys_step.cuh) chosen by the same rule, so a domain advanced in a batch is
+// bit-identical to the same domain advanced alone.
 //
 // Persistent mode.  A grid of co-resident blocks (cooperative launch) walks
 // the tile list grid-stride, then meets at a grid barrier before the next
@@ -56,8 +58,12 @@ __device__ __forceinline__ void batch_tile(const BatchDomain& D, uint32_t local,
   for (int k = 0; k < nzt; ++k) {
     const int z = tz * nzt + k;
     if (z >= D.p.g.nz) break;
-    step_row<PREC, COLL, false, false, WM, P>(D.p, D.pop, D.flags, D.links, D.rho, D.u, status,
-                                              tx * 32, y, z);
+    if (D.pairs)  // uniform over the block
+      step_row2<PREC, COLL, false, false, WM, P>(D.p, D.pop, D.flags, D.links, D.rho, D.u, status,
+                                                 tx * 64, y, z);
+    else
+      step_row<PREC, COLL, false, false, WM, P>(D.p, D.pop, D.flags, D.links, D.rho, D.u, status,
+                                                tx * 32, y, z);
   }
 }
 

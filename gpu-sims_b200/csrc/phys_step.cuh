@@ -82,6 +82,36 @@ __device__ __forceinline__ float wall_term(const PhysParams& p, int x, int y, in
   return 6.0f * wf(J) * cu;
 }
 
+// Arithmetic policies for the collision.  Every operation is an explicitly
+// rounded intrinsic (no compiler contraction), so the one-node policy and
+// the two-node policy built on Blackwell's packed fp32 instructions
+// (FADD2/FMUL2/FFMA2: one instruction for two lanes' values) evaluate the
+// same operation graph and give bit-identical populations.
+struct Ops1 {
+  using F = float;
+  static __device__ __forceinline__ F splat(float c) { return c; }
+  static __device__ __forceinline__ F add(F a, F b) { return __fadd_rn(a, b); }
+  static __device__ __forceinline__ F sub(F a, F b) { return __fsub_rn(a, b); }
+  static __device__ __forceinline__ F mul(F a, F b) { return __fmul_rn(a, b); }
+  static __device__ __forceinline__ F fma(F a, F b, F c) { return __fmaf_rn(a, b, c); }
+  static __device__ __forceinline__ F div(F a, F b) { return __fdiv_rn(a, b); }
+  static __device__ __forceinline__ F sqrt(F a) { return __fsqrt_rn(a); }
+};
+struct Ops2 {
+  using F = float2;
+  static __device__ __forceinline__ F splat(float c) { return make_float2(c, c); }
+  static __device__ __forceinline__ F add(F a, F b) { return __fadd2_rn(a, b); }
+  // a - b as b * (-1) + a: the product is exact, so the single rounding
+  // equals that of a - b.
+  static __device__ __forceinline__ F sub(F a, F b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+  static __device__ __forceinline__ F mul(F a, F b) { return __fmul2_rn(a, b); }
+  static __device__ __forceinline__ F fma(F a, F b, F c) { return __ffma2_rn(a, b, c); }
+  static __device__ __forceinline__ F div(F a, F b) {
+    return make_float2(__fdiv_rn(a.x, b.x), __fdiv_rn(a.y, b.y));
+  }
+  static __device__ __forceinline__ F sqrt(F a) { return make_float2(__fsqrt_rn(a.x), __fsqrt_rn(a.y)); }
+};
+
 // Collision on shifted populations in storage units v = SC (f - w), in
 // place, written per opposite pair (a, b): with cu = c_a . u the equilibrium
 // splits into an even part  w (drho + rho (4.5 cu^2 - 1.5 u.u))  shared by a
@@ -93,101 +123,142 @@ __device__ __forceinline__ float wall_term(const PhysParams& p, int x, int y, in
 // with h = (omega + omega-)/2, k = (omega - omega-)/2, E = omega even +
 // (1 - omega/2) even source, O = omega- odd + (1 - omega-/2) odd source.
 // Returns rho and the force-shifted velocity u = (sum c f + F/2) / rho.
-template <int COLL, bool SMAG, bool FORCE, int PREC>
-__device__ __forceinline__ void collide(const PhysParams& p, float (&g)[Q], float& rho_out,
-                                        float& ux, float& uy, float& uz) {
+// O is Ops1 (one node) or Ops2 (two nodes in the .x/.y lanes).
+template <class O, int COLL, bool SMAG, bool FORCE, int PREC>
+__device__ __forceinline__ void collide_t(const PhysParams& p, typename O::F (&g)[Q],
+                                          typename O::F& rho_out, typename O::F& ux,
+                                          typename O::F& uy, typename O::F& uz) {
+  using F = typename O::F;
   constexpr float SC = Store<PREC>::SC, INV = Store<PREC>::INV;
   constexpr float WF = 1.0f / 18.0f, WE = 1.0f / 36.0f, W0 = 1.0f / 3.0f;
-  float drs = g[0], jx = 0.0f, jy = 0.0f, jz = 0.0f;  // sums in storage units
+  F drs = g[0], jx = O::splat(0.f), jy = O::splat(0.f), jz = O::splat(0.f);
   static_for<0, 9>([&](auto PI) {
     constexpr int a = pair_a(decltype(PI)::value), b = pair_b(decltype(PI)::value);
-    const float d = g[a] - g[b];
-    drs += g[a] + g[b];
-    if (cx(a)) jx += cx(a) * d;
-    if (cy(a)) jy += cy(a) * d;
-    if (cz(a)) jz += cz(a) * d;
+    const F d = O::sub(g[a], g[b]);
+    drs = O::add(drs, O::add(g[a], g[b]));
+    if (cx(a) > 0) jx = O::add(jx, d);
+    if (cy(a) > 0) jy = O::add(jy, d);
+    if (cy(a) < 0) jy = O::sub(jy, d);
+    if (cz(a) > 0) jz = O::add(jz, d);
+    if (cz(a) < 0) jz = O::sub(jz, d);
   });
-  const float rho = fmaf(drs, INV, 1.0f);
-  const float js = INV / rho;
-  ux = jx * js;
-  uy = jy * js;
-  uz = jz * js;
+  const F rho = O::fma(drs, O::splat(INV), O::splat(1.0f));
+  const F js = O::div(O::splat(INV), rho);
+  ux = O::mul(jx, js);
+  uy = O::mul(jy, js);
+  uz = O::mul(jz, js);
   if (FORCE) {
-    ux = fmaf(0.5f, p.accel[0], ux);
-    uy = fmaf(0.5f, p.accel[1], uy);
-    uz = fmaf(0.5f, p.accel[2], uz);
+    ux = O::add(ux, O::splat(0.5f * p.accel[0]));
+    uy = O::add(uy, O::splat(0.5f * p.accel[1]));
+    uz = O::add(uz, O::splat(0.5f * p.accel[2]));
   }
   rho_out = rho;
-  const float uu15 = 1.5f * (ux * ux + uy * uy + uz * uz);
-  const float sr = SC * rho;
+  const F uu15 = O::mul(O::splat(1.5f), O::fma(ux, ux, O::fma(uy, uy, O::mul(uz, uz))));
+  const F sr = O::mul(O::splat(SC), rho);
 
-  float omega = p.omega;
+  F omega = O::splat(p.omega);
   if (SMAG) {
     // Pi = sum c c (f - feq) (even in c: pair sums suffice); Hou et al. (1996)
     //   tau_eff = (tau + sqrt(tau^2 + 18 sqrt(2) Cs^2 |Pi| / rho)) / 2.
-    float pxx = 0.f, pyy = 0.f, pzz = 0.f, pxy = 0.f, pxz = 0.f, pyz = 0.f;
+    F pxx = O::splat(0.f), pyy = pxx, pzz = pxx, pxy = pxx, pxz = pxx, pyz = pxx;
     static_for<0, 9>([&](auto PI) {
       constexpr int a = pair_a(decltype(PI)::value), b = pair_b(decltype(PI)::value);
       constexpr float w = wf(a);
-      const float cu = cx(a) * ux + cy(a) * uy + cz(a) * uz;
-      const float even = fmaf(w * sr, fmaf(4.5f * cu, cu, -uu15), w * drs);
-      const float ne = (g[a] + g[b]) - 2.0f * even;
-      if (cx(a)) pxx += ne;
-      if (cy(a)) pyy += ne;
-      if (cz(a)) pzz += ne;
-      if (cx(a) * cy(a)) pxy += cx(a) * cy(a) * ne;
-      if (cx(a) * cz(a)) pxz += cx(a) * cz(a) * ne;
-      if (cy(a) * cz(a)) pyz += cy(a) * cz(a) * ne;
+      F cu = O::splat(0.f);
+      if (cx(a)) cu = ux;
+      if (cy(a) > 0) cu = cx(a) ? O::add(cu, uy) : uy;
+      if (cy(a) < 0) cu = cx(a) ? O::sub(cu, uy) : O::sub(O::splat(0.f), uy);
+      if (cz(a) > 0) cu = (cx(a) || cy(a)) ? O::add(cu, uz) : uz;
+      if (cz(a) < 0) cu = (cx(a) || cy(a)) ? O::sub(cu, uz) : O::sub(O::splat(0.f), uz);
+      const F t = O::fma(O::mul(O::splat(4.5f), cu), cu, O::sub(O::splat(0.f), uu15));
+      const F even = O::fma(O::mul(O::splat(w), sr), t, O::mul(O::splat(w), drs));
+      const F ne = O::fma(O::splat(-2.0f), even, O::add(g[a], g[b]));
+      if (cx(a)) pxx = O::add(pxx, ne);
+      if (cy(a)) pyy = O::add(pyy, ne);
+      if (cz(a)) pzz = O::add(pzz, ne);
+      if (cx(a) * cy(a) > 0) pxy = O::add(pxy, ne);
+      if (cx(a) * cy(a) < 0) pxy = O::sub(pxy, ne);
+      if (cx(a) * cz(a) > 0) pxz = O::add(pxz, ne);
+      if (cx(a) * cz(a) < 0) pxz = O::sub(pxz, ne);
+      if (cy(a) * cz(a) > 0) pyz = O::add(pyz, ne);
+      if (cy(a) * cz(a) < 0) pyz = O::sub(pyz, ne);
     });
-    const float pn = INV * sqrtf(pxx * pxx + pyy * pyy + pzz * pzz +
-                                 2.0f * (pxy * pxy + pxz * pxz + pyz * pyz));
+    const F off = O::fma(pxy, pxy, O::fma(pxz, pxz, O::mul(pyz, pyz)));
+    const F q = O::fma(pxx, pxx, O::fma(pyy, pyy, O::fma(pzz, pzz, O::mul(O::splat(2.f), off))));
+    const F pn = O::mul(O::splat(INV), O::sqrt(q));
     const float cs2 = p.smag_cs * p.smag_cs;
-    const float tau_eff = 0.5f * (p.tau + sqrtf(fmaf(p.tau, p.tau, 25.455844f * cs2 * pn / rho)));
-    omega = 1.0f / tau_eff;
+    const F arg = O::fma(O::splat(p.tau), O::splat(p.tau),
+                         O::div(O::mul(O::splat(25.455844f * cs2), pn), rho));
+    const F tau_eff = O::mul(O::splat(0.5f), O::add(O::splat(p.tau), O::sqrt(arg)));
+    omega = O::div(O::splat(1.0f), tau_eff);
   }
-  const float omega_m =
-      COLL == LBM_COLL_BGK ? omega : 1.0f / (p.trt_magic / (1.0f / omega - 0.5f) + 0.5f);
-  const float h = 0.5f * (omega + omega_m), k = 0.5f * (omega - omega_m);
-  const float c1 = 1.0f - h;
-  // per weight class: omega w SC rho, omega w drs, 3 omega- w SC rho, source factors
-  const float erF = omega * WF * sr, erE = omega * WE * sr;
-  const float edF = omega * WF * drs, edE = omega * WE * drs;
-  const float orF = 3.0f * omega_m * WF * sr, orE = 3.0f * omega_m * WE * sr;
-  float ua3 = 0.f, ksF = 0.f, ksE = 0.f, kaF = 0.f, kaE = 0.f;
+  F omega_m = omega;
+  if (COLL == LBM_COLL_TRT)
+    omega_m = O::div(O::splat(1.0f),
+                     O::add(O::div(O::splat(p.trt_magic),
+                                   O::sub(O::div(O::splat(1.0f), omega), O::splat(0.5f))),
+                            O::splat(0.5f)));
+  const F h = O::mul(O::splat(0.5f), O::add(omega, omega_m));
+  const F k = O::mul(O::splat(0.5f), O::sub(omega, omega_m));
+  const F c1 = O::sub(O::splat(1.0f), h);
+  // per weight class: omega w SC rho, omega w drs, 3 omega- w SC rho
+  const F osr = O::mul(omega, sr), ods = O::mul(omega, drs), omsr = O::mul(omega_m, sr);
+  const F erF = O::mul(O::splat(WF), osr), erE = O::mul(O::splat(WE), osr);
+  const F edF = O::mul(O::splat(WF), ods), edE = O::mul(O::splat(WE), ods);
+  const F orF = O::mul(O::splat(3.0f * WF), omsr), orE = O::mul(O::splat(3.0f * WE), omsr);
+  F ua3 = O::splat(0.f), ksF = ua3, ksE = ua3, kaF = ua3, kaE = ua3;
   if (FORCE) {
-    ua3 = 3.0f * (ux * p.accel[0] + uy * p.accel[1] + uz * p.accel[2]);
-    const float fp = 1.0f - 0.5f * omega, fm = 1.0f - 0.5f * omega_m;
-    ksF = fp * WF * sr;
-    ksE = fp * WE * sr;
-    kaF = 3.0f * fm * WF * sr;
-    kaE = 3.0f * fm * WE * sr;
+    ua3 = O::mul(O::splat(3.0f),
+                 O::fma(ux, O::splat(p.accel[0]), O::fma(uy, O::splat(p.accel[1]),
+                                                        O::mul(uz, O::splat(p.accel[2])))));
+    const F fpsr = O::mul(O::fma(O::splat(-0.5f), omega, O::splat(1.0f)), sr);
+    const F fmsr = O::mul(O::fma(O::splat(-0.5f), omega_m, O::splat(1.0f)), sr);
+    ksF = O::mul(O::splat(WF), fpsr);
+    ksE = O::mul(O::splat(WE), fpsr);
+    kaF = O::mul(O::splat(3.0f * WF), fmsr);
+    kaE = O::mul(O::splat(3.0f * WE), fmsr);
   }
   {
-    float e0 = fmaf(-omega * W0 * sr, uu15, omega * W0 * drs);
-    if (FORCE) e0 = fmaf(-(1.0f - 0.5f * omega) * W0 * sr, ua3, e0);
-    g[0] = fmaf(1.0f - omega, g[0], e0);
+    F e0 = O::fma(O::sub(O::splat(0.f), O::mul(O::splat(W0), osr)), uu15, O::mul(O::splat(W0), ods));
+    if (FORCE)
+      e0 = O::fma(O::sub(O::splat(0.f), O::mul(O::splat(W0), O::mul(O::fma(O::splat(-0.5f), omega,
+                                                                          O::splat(1.0f)), sr))),
+                  ua3, e0);
+    g[0] = O::fma(O::sub(O::splat(1.0f), omega), g[0], e0);
   }
   static_for<0, 9>([&](auto PI) {
     constexpr int a = pair_a(decltype(PI)::value), b = pair_b(decltype(PI)::value);
     constexpr bool face = (a <= 6);
-    const float cu = cx(a) * ux + cy(a) * uy + cz(a) * uz;
-    const float t = fmaf(4.5f * cu, cu, -uu15);
-    float E = fmaf(face ? erF : erE, t, face ? edF : edE);
-    float O = (face ? orF : orE) * cu;
+    F cu = O::splat(0.f);
+    if (cx(a)) cu = ux;
+    if (cy(a) > 0) cu = cx(a) ? O::add(cu, uy) : uy;
+    if (cy(a) < 0) cu = cx(a) ? O::sub(cu, uy) : O::sub(O::splat(0.f), uy);
+    if (cz(a) > 0) cu = (cx(a) || cy(a)) ? O::add(cu, uz) : uz;
+    if (cz(a) < 0) cu = (cx(a) || cy(a)) ? O::sub(cu, uz) : O::sub(O::splat(0.f), uz);
+    const F t = O::fma(O::mul(O::splat(4.5f), cu), cu, O::sub(O::splat(0.f), uu15));
+    F E = O::fma(face ? erF : erE, t, face ? edF : edE);
+    F Od = O::mul(face ? orF : orE, cu);
     if (FORCE) {
       const float ca = cx(a) * p.accel[0] + cy(a) * p.accel[1] + cz(a) * p.accel[2];
-      E = fmaf(face ? ksF : ksE, fmaf(9.0f * ca, cu, -ua3), E);
-      O = fmaf(face ? kaF : kaE, ca, O);
+      E = O::fma(face ? ksF : ksE, O::fma(O::splat(9.0f * ca), cu, O::sub(O::splat(0.f), ua3)), E);
+      Od = O::fma(face ? kaF : kaE, O::splat(ca), Od);
     }
-    const float ga = g[a], gb = g[b];
+    const F ga = g[a], gb = g[b];
     if (COLL == LBM_COLL_BGK) {
-      g[a] = fmaf(c1, ga, E + O);
-      g[b] = fmaf(c1, gb, E - O);
+      g[a] = O::fma(c1, ga, O::add(E, Od));
+      g[b] = O::fma(c1, gb, O::sub(E, Od));
     } else {
-      g[a] = fmaf(c1, ga, fmaf(-k, gb, E + O));
-      g[b] = fmaf(c1, gb, fmaf(-k, ga, E - O));
+      const F mk = O::sub(O::splat(0.f), k);
+      g[a] = O::fma(c1, ga, O::fma(mk, gb, O::add(E, Od)));
+      g[b] = O::fma(c1, gb, O::fma(mk, ga, O::sub(E, Od)));
     }
   });
+}
+
+template <int COLL, bool SMAG, bool FORCE, int PREC>
+__device__ __forceinline__ void collide(const PhysParams& p, float (&g)[Q], float& rho_out,
+                                        float& ux, float& uy, float& uz) {
+  collide_t<Ops1, COLL, SMAG, FORCE, PREC>(p, g, rho_out, ux, uy, uz);
 }
 
 // Launch shape of the step kernel: a block is 32 x STEP_BY nodes of one
@@ -378,6 +449,209 @@ __device__ __forceinline__ void step_row(const PhysParams& p, void* __restrict__
       const bool left_ok = __shfl_up_sync(FULL, pass, 1) && lane > 0;
       if (left_ok) S::raw_st(sP, ln + offs<0, DY, DZ>(G, w), from_left);
       if (fluid && edge) S::raw_st(sP, ln + offs<1, DY, DZ>(G, w), g[a]);
+    }
+  });
+}
+
+// Two nodes per thread (step_row2) need an even row length, so that pairs
+// never straddle a row and vector accesses stay aligned, and pay off when the
+// rows fill the 64-wide warps: measured on B200 a two-node lane does the work
+// of about 1.25 one-node lanes, so pairs are used when
+// 1.25 * nx / (64 ceil(nx/64)) >= nx / (32 ceil(nx/32)).
+__host__ __device__ inline bool step_pairs(int nx) {
+#ifdef LBM_NO_PAIRS
+  return false;
+#else
+  if (nx % 2) return false;
+  const int w64 = 64 * ((nx + 63) / 64), w32 = 32 * ((nx + 31) / 32);
+  return 5 * w32 >= 4 * w64;
+#endif
+}
+
+// Vector access to two x-adjacent slots (x even, so 8- or 4-byte aligned).
+template <int PREC> struct Vec2;
+template <> struct Vec2<LBM_PREC_F32> {
+  using V = float2;
+  static __device__ __forceinline__ V ld(const float* p, uint32_t i) { return *reinterpret_cast<const float2*>(p + i); }
+  static __device__ __forceinline__ void st(float* p, uint32_t i, float a, float b) {
+    *reinterpret_cast<float2*>(p + i) = make_float2(a, b);
+  }
+  static __device__ __forceinline__ float lo(V v) { return v.x; }
+  static __device__ __forceinline__ float hi(V v) { return v.y; }
+};
+template <> struct Vec2<LBM_PREC_F16S> {
+  using V = __half2;
+  static __device__ __forceinline__ V ld(const __half* p, uint32_t i) { return *reinterpret_cast<const __half2*>(p + i); }
+  static __device__ __forceinline__ void st(__half* p, uint32_t i, float a, float b) {
+    *reinterpret_cast<__half2*>(p + i) = __floats2half2_rn(a, b);
+  }
+  static __device__ __forceinline__ float lo(V v) { return __low2float(v); }
+  static __device__ __forceinline__ float hi(V v) { return __high2float(v); }
+};
+template <> struct Vec2<LBM_PREC_BF16S> {
+  using V = __nv_bfloat162;
+  static __device__ __forceinline__ V ld(const __nv_bfloat16* p, uint32_t i) {
+    return *reinterpret_cast<const __nv_bfloat162*>(p + i);
+  }
+  static __device__ __forceinline__ void st(__nv_bfloat16* p, uint32_t i, float a, float b) {
+    *reinterpret_cast<__nv_bfloat162*>(p + i) = __floats2bfloat162_rn(a, b);
+  }
+  static __device__ __forceinline__ float lo(V v) { return __low2float(v); }
+  static __device__ __forceinline__ float hi(V v) { return __high2float(v); }
+};
+
+// The step of step_row for two nodes per thread: lane l of the warp updates
+// x = x0 + 2l (node A) and x + 1 (node B) (nx even, so both exist or neither
+// does); a warp covers 64 consecutive x.  Every slot pair (x, x+1) moves as
+// one vector access; the slots at x+1 / x+2 of the c_x = +1 pairs come from
+// the lane's own vector and the next lane's by shuffle, the row's last pair
+// touching x+2 itself.  The two nodes collide together in the lanes of
+// packed fp32 instructions (Ops2).  Solid nodes are never written (their
+// slots hold neighbours' bounce-back values), so a pair with a solid node
+// stores element-wise.
+template <int PREC, int COLL, bool SMAG, bool FORCE, bool WRITE_MOMENTS, int P>
+__device__ __forceinline__ void step_row2(const PhysParams& p, void* __restrict__ pop_v,
+                                          const uint8_t* __restrict__ flags,
+                                          const uint32_t* __restrict__ links,
+                                          float* __restrict__ rho_o, float* __restrict__ u_o,
+                                          unsigned* __restrict__ status, const int x0, const int y,
+                                          const int z) {
+  using S = Store<PREC>;
+  using V2 = Vec2<PREC>;
+  using T = typename S::T;
+  const PhysGeom& G = p.g;
+  const int lane = threadIdx.x & 31;
+  const int xa = x0 + 2 * lane;
+  const bool valid = xa < G.nx;
+  const int xc = valid ? xa : G.nx - 2;
+  const bool edge = (lane == 31) || (xa + 2 >= G.nx);  // its node B touches x+2 itself
+  const uint32_t N = (uint32_t)G.n;
+  const uint32_t nid = (uint32_t)xc + (uint32_t)G.nx * ((uint32_t)y + (uint32_t)G.ny * (uint32_t)z);
+  T* pop = reinterpret_cast<T*>(pop_v);
+  const size_t SS = G.slot_stride;
+  const uint32_t lnA = lin32(G, xc, y, z);
+  const uint32_t lnB = lnA + 1;
+  const Wrap w = wrap_terms(G, xc, y, z);       // y/z terms; node A is never at x = nx-1
+  const Wrap wB = wrap_terms(G, xc + 1, y, z);  // x term of node B
+  const bool xloA = !G.per[0] && xc == 0, xhiB = !G.per[0] && xc + 1 == G.nx - 1;
+  const bool ylo = !G.per[1] && y == 0, yhi = !G.per[1] && y == G.ny - 1;
+  const bool zlo = !G.per[2] && z == 0, zhi = !G.per[2] && z == G.nz - 1;
+  const bool moving = p.any_moving_wall;
+
+  const uint16_t fl2 = valid ? *reinterpret_cast<const uint16_t*>(flags + nid) : (uint16_t)0x0101u;
+  const uint8_t flA = (uint8_t)(fl2 & 0xffu), flB = (uint8_t)(fl2 >> 8);
+  float2 g2[Q];  // .x = node A, .y = node B
+  {
+    const typename V2::V r = V2::ld(pop, lnA);
+    g2[0] = make_float2(V2::lo(r), V2::hi(r));
+  }
+  static_for<0, 9>([&](auto PI) {
+    constexpr int pi = decltype(PI)::value;
+    constexpr int a = pair_a(pi), b = pair_b(pi);
+    constexpr int DX = cx(a), DY = cy(a), DZ = cz(a);
+    const T* s0 = pop + (size_t)(1 + 2 * pi) * SS;
+    const T* sP = P ? s0 + SS : s0;
+    const T* sQ = P ? s0 : s0 + SS;
+    const bool yz_fwd = (DY > 0 && yhi) || (DY < 0 && ylo) || (DZ > 0 && zhi) || (DZ < 0 && zlo);
+    const bool yz_bwd = (DY > 0 && ylo) || (DY < 0 && yhi) || (DZ > 0 && zlo) || (DZ < 0 && zhi);
+    // f_a of both nodes from X = S[1-P](x, x+1); S[P] across a wall
+    const typename V2::V xv = V2::ld(yz_bwd ? sP : sQ, lnA);
+    g2[a] = make_float2(V2::lo(xv), V2::hi(xv));
+    if (DX > 0 && xloA) g2[a].x = S::raw_ld(sP, lnA);  // node A at the -x wall
+    // f_b from Y = S[P](n + d); S[1-P] across a wall
+    const typename V2::V yv = V2::ld(yz_fwd ? sQ : sP, lnA + offs<0, DY, DZ>(G, w));
+    if (DX == 0) {
+      g2[b] = make_float2(V2::lo(yv), V2::hi(yv));
+    } else {
+      float nxt = __shfl_down_sync(FULL, V2::lo(yv), 1);  // x + 2
+      if (edge) nxt = S::raw_ld((yz_fwd || xhiB) ? sQ : sP, lnB + offs<1, DY, DZ>(G, wB));
+      g2[b] = make_float2(V2::hi(yv), nxt);  // x + 1, x + 2
+    }
+  });
+  if (moving) {
+    static_for<0, 9>([&](auto PI) {
+      constexpr int pi = decltype(PI)::value;
+      constexpr int a = pair_a(pi), b = pair_b(pi);
+      constexpr int DX = cx(a), DY = cy(a), DZ = cz(a);
+      const bool yz_fwd = (DY > 0 && yhi) || (DY < 0 && ylo) || (DZ > 0 && zhi) || (DZ < 0 && zlo);
+      const bool yz_bwd = (DY > 0 && ylo) || (DY < 0 && yhi) || (DZ > 0 && zlo) || (DZ < 0 && zhi);
+      if (yz_bwd || (DX > 0 && xloA)) g2[a].x = fmaf(S::SC, wall_term<a>(p, xc, y, z), g2[a].x);
+      if (yz_fwd) g2[b].x = fmaf(S::SC, wall_term<b>(p, xc, y, z), g2[b].x);
+      if (yz_bwd) g2[a].y = fmaf(S::SC, wall_term<a>(p, xc + 1, y, z), g2[a].y);
+      if (yz_fwd || (DX > 0 && xhiB)) g2[b].y = fmaf(S::SC, wall_term<b>(p, xc + 1, y, z), g2[b].y);
+    });
+  }
+  const bool fluidA = valid && !(flA & FLAG_SOLID);
+  const bool fluidB = valid && !(flB & FLAG_SOLID);
+  auto solid_fix = [&](auto lane_sel, uint32_t nidn, uint32_t ln, const Wrap& wn, bool xlo, bool xhi) {
+    constexpr bool B = decltype(lane_sel)::value != 0;
+    auto at = [&](int i) -> float& { return B ? g2[i].y : g2[i].x; };
+    const uint32_t L = links[nidn];
+    static_for<0, 9>([&](auto PI) {
+      constexpr int pi = decltype(PI)::value;
+      constexpr int a = pair_a(pi), b = pair_b(pi);
+      constexpr int DX = cx(a), DY = cy(a), DZ = cz(a);
+      const T* s0 = pop + (size_t)(1 + 2 * pi) * SS;
+      const T* sP = P ? s0 + SS : s0;
+      const T* sQ = P ? s0 : s0 + SS;
+      const bool fwd_wall = (DX > 0 && xhi) || (DY > 0 && yhi) || (DY < 0 && ylo) || (DZ > 0 && zhi) ||
+                            (DZ < 0 && zlo);
+      const bool bwd_wall =
+          (DX > 0 && xlo) || (DY > 0 && ylo) || (DY < 0 && yhi) || (DZ > 0 && zlo) || (DZ < 0 && zhi);
+      if (((L >> b) & 1u) && !bwd_wall) at(a) = S::raw_ld(sP, ln);
+      if (((L >> a) & 1u) && !fwd_wall) at(b) = S::raw_ld(sQ, ln + offs<DX, DY, DZ>(G, wn));
+    });
+  };
+  if (fluidA && (flA & FLAG_SOLID_LINK)) solid_fix(IC<0>{}, nid, lnA, w, xloA, false);
+  if (fluidB && (flB & FLAG_SOLID_LINK)) solid_fix(IC<1>{}, nid + 1, lnB, wB, false, xhiB);
+
+  float2 r2, ux2, uy2, uz2;
+  collide_t<Ops2, COLL, SMAG, FORCE, PREC>(p, g2, r2, ux2, uy2, uz2);
+
+  if (WRITE_MOMENTS && valid) {
+    *reinterpret_cast<float2*>(rho_o + nid) = make_float2(fluidA ? r2.x : 0.f, fluidB ? r2.y : 0.f);
+    *reinterpret_cast<float2*>(u_o + nid) = make_float2(fluidA ? ux2.x : 0.f, fluidB ? ux2.y : 0.f);
+    *reinterpret_cast<float2*>(u_o + N + nid) = make_float2(fluidA ? uy2.x : 0.f, fluidB ? uy2.y : 0.f);
+    *reinterpret_cast<float2*>(u_o + 2 * N + nid) = make_float2(fluidA ? uz2.x : 0.f, fluidB ? uz2.y : 0.f);
+    const bool badA = fluidA && (!(r2.x > 0.f) || !isfinite(r2.x) || !isfinite(ux2.x) ||
+                                 !isfinite(uy2.x) || !isfinite(uz2.x));
+    const bool badB = fluidB && (!(r2.y > 0.f) || !isfinite(r2.y) || !isfinite(ux2.y) ||
+                                 !isfinite(uy2.y) || !isfinite(uz2.y));
+    if (badA || badB) atomicOr(status, 1u);
+  }
+
+  const bool both = fluidA && fluidB;
+  // store node A / node B values at slot positions i (A) and i+1 (B)
+  auto st2 = [&](T* arr, uint32_t i, float va, float vb) {
+    if (both) V2::st(arr, i, va, vb);
+    else {
+      if (fluidA) S::raw_st(arr, i, va);
+      if (fluidB) S::raw_st(arr, i + 1, vb);
+    }
+  };
+  st2(pop, lnA, g2[0].x, g2[0].y);
+  const bool passB = fluidB && !edge;  // node B's Y value at x+2 is stored by lane+1
+  static_for<0, 9>([&](auto PI) {
+    constexpr int pi = decltype(PI)::value;
+    constexpr int a = pair_a(pi), b = pair_b(pi);
+    constexpr int DX = cx(a), DY = cy(a), DZ = cz(a);
+    T* s0 = pop + (size_t)(1 + 2 * pi) * SS;
+    T* sP = P ? s0 + SS : s0;
+    T* sQ = P ? s0 : s0 + SS;
+    st2(sQ, lnA, g2[b].x, g2[b].y);  // f*_b -> X = S[1-P](n)
+    if (DX == 0) {
+      st2(sP, lnA + offs<0, DY, DZ>(G, w), g2[a].x, g2[a].y);  // f*_a -> Y = S[P](n+d)
+    } else {
+      // aligned pair (x, x+1) of row (y+dy, z+dz): x from lane-1's node B, x+1 from node A
+      const float from_left = __shfl_up_sync(FULL, g2[a].y, 1);
+      const bool left_ok = __shfl_up_sync(FULL, passB, 1) && lane > 0;
+      const uint32_t i = lnA + offs<0, DY, DZ>(G, w);
+      if (left_ok && fluidA) V2::st(sP, i, from_left, g2[a].x);
+      else {
+        if (left_ok) S::raw_st(sP, i, from_left);
+        if (fluidA) S::raw_st(sP, i + 1, g2[a].x);
+      }
+      if (fluidB && edge) S::raw_st(sP, lnB + offs<1, DY, DZ>(G, wB), g2[a].y);
     }
   });
 }

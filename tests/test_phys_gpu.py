@@ -2,7 +2,7 @@
 shifted populations) against the textbook FP64 stream-collide oracle.
 
 Tolerances (written per test): after a few hundred steps fp32 rounding
-leaves |du| below 1e-5 of the velocity scale and |drho| below 1e-5 (fp32
+leaves |du| below 3e-5 of the velocity scale and |drho| below 1e-5 (fp32
 storage); reduced-precision storage is held to the relative L2 velocity
 error the precision allows."""
 import numpy as np
@@ -37,7 +37,7 @@ def make_pair(lbm, oracle, shape, periodic=(0, 0, 0), tau=0.6, collision=0, smag
     return lat, st
 
 
-def compare(lat, st, tol_u=1e-5, tol_rho=1e-5):
+def compare(lat, st, tol_u=3e-5, tol_rho=1e-5):
     rho, u = lat.read_moments()
     scale = max(np.abs(st.u).max(), 1e-12)
     du = np.max(np.abs(u.T - st.u)) / scale
@@ -68,9 +68,8 @@ def test_lid_driven_cavity(gpu, oracle):
     lat.close()
 
 
-@pytest.mark.parametrize("coll", [0, 1])
-def test_channel_sphere_force(gpu, oracle, coll):
-    shape = (48, 16, 16)
+@pytest.mark.parametrize("coll,shape", [(0, (48, 16, 16)), (1, (64, 16, 16)), (0, (47, 16, 16))])
+def test_channel_sphere_force(gpu, oracle, coll, shape):
     mask = sphere_mask(shape, (16, 8, 8), 4)
     rng = np.random.default_rng(1234)
     u = 1e-3 * rng.standard_normal((3, int(np.prod(shape))))
@@ -93,10 +92,11 @@ def test_taylor_green_periodic(gpu, oracle, coll, smag):
     lat.close()
 
 
-def test_mixed_faces_and_solids(gpu, oracle):
+@pytest.mark.parametrize("shape", [(20, 14, 11), (21, 14, 11), (66, 5, 4), (128, 6, 5)])
+def test_mixed_faces_and_solids(gpu, oracle, shape):
     """Periodic y only, walls elsewhere, two moving faces, scattered solids
-    touching the walls: exercises every ghost-slot path."""
-    shape = (20, 14, 11)
+    touching the walls: exercises every ghost-slot path, with one node per
+    thread (odd or short rows) and two (rows filling 64-wide warps)."""
     n = int(np.prod(shape))
     rng = np.random.default_rng(4)
     mask = (rng.random(n) < 0.08).astype(np.uint8)
