@@ -8,6 +8,7 @@ nvcc cross-compiles for sm_100a without a GPU.
 from __future__ import annotations
 
 import argparse
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -57,18 +58,24 @@ def build(force: bool = False, verbose: bool = False, out: Path | None = None,
     BUILD.mkdir(parents=True, exist_ok=True)
     OUT.parent.mkdir(parents=True, exist_ok=True)
     cc = nvcc()
-    objs = []
+    objs, cmds = [], []
     for src in sources():
         obj = BUILD / (src.name + ".o")
         objs.append(obj)
         if not force and not _stale(obj, src):
             continue
-        cmd = [cc, "-c", str(src), "-o", str(obj)] + CUDA_FLAGS + extra + HOST_EXTRA.get(src.name, [])
-        if src.suffix == ".cpp":
-            cmd = [cc, "-x", "cu", "-c", str(src), "-o", str(obj)] + CUDA_FLAGS + extra + HOST_EXTRA.get(src.name, [])
-        if verbose:
-            print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
+        lang = ["-x", "cu"] if src.suffix == ".cpp" else []
+        cmds.append([cc] + lang + ["-c", str(src), "-o", str(obj)] + CUDA_FLAGS + extra +
+                    HOST_EXTRA.get(src.name, []))
+    # translation units compile in parallel (the step kernels dominate)
+    with concurrent.futures.ThreadPoolExecutor(max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for cmd in cmds:
+            if verbose:
+                print(" ".join(cmd), flush=True)
+        for r in ex.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds):
+            if r.returncode:
+                sys.stderr.write(r.stdout + r.stderr)
+                raise subprocess.CalledProcessError(r.returncode, r.args)
     if force or not OUT.exists() or any(o.stat().st_mtime > OUT.stat().st_mtime for o in objs):
         cmd = [cc, "-shared", "-o", str(OUT)] + [str(o) for o in objs] + ARCH
         if verbose:

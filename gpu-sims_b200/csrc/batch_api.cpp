@@ -31,6 +31,8 @@ struct lbm_batch {
   std::vector<void*> allocs;
   lbm::BatchDomain* d_dom = nullptr;
   std::vector<lbm::BatchDomain> h_dom;
+  uint2* d_tiles = nullptr;  // per tile: (domain, index within the domain)
+  size_t tiles_cap = 0;
   unsigned* status = nullptr;
   unsigned* bar = nullptr;
   uint32_t ntiles = 0;
@@ -87,6 +89,7 @@ void drop_graphs(lbm_batch* b) {
 lbm::BatchLaunch launch_of(const lbm_batch* b) {
   lbm::BatchLaunch L{};
   L.dom = b->d_dom;
+  L.tiles = b->d_tiles;
   L.ndom = (int)b->dom.size();
   L.ntiles = b->ntiles;
   L.rows = b->sched.rows_per_block;
@@ -114,7 +117,7 @@ int build_tiles(lbm_batch* b) {
     D.links = v.links;
     D.rho = v.rho;
     D.u = v.u;
-    D.pairs = lbm::step_pairs_host(v.d.nx) ? 1u : 0u;
+    D.pairs = (LBM_BATCH_PAIRS && lbm::step_pairs_host(v.d.nx)) ? 1u : 0u;
     D.tiles_x = D.pairs ? (v.d.nx + 63) / 64 : (v.d.nx + 31) / 32;
     D.tiles_y = (v.d.ny + R - 1) / R;
     D.tile_begin = (uint32_t)t;
@@ -122,6 +125,25 @@ int build_tiles(lbm_batch* b) {
   }
   if (t >= (1ull << 31)) return bfail(b, LBM_ERR_UNSUPPORTED, "more than 2^31 tiles");
   b->ntiles = (uint32_t)t;
+  std::vector<uint2> table(t);
+  for (size_t i = 0; i < b->dom.size(); ++i) {
+    const uint32_t begin = b->h_dom[i].tile_begin;
+    const uint32_t end = i + 1 < b->dom.size() ? b->h_dom[i + 1].tile_begin : (uint32_t)t;
+    for (uint32_t k = begin; k < end; ++k) table[k] = make_uint2((unsigned)i, k - begin);
+  }
+  if (b->tiles_cap < t) {
+    if (b->d_tiles) {
+      cudaFree(b->d_tiles);
+      b->allocs.erase(std::find(b->allocs.begin(), b->allocs.end(), (void*)b->d_tiles));
+      b->d_tiles = nullptr;
+    }
+    void* p = nullptr;
+    if (int rc = balloc(b, &p, t * sizeof(uint2), "cudaMalloc(tile table)")) return rc;
+    b->d_tiles = static_cast<uint2*>(p);
+    b->tiles_cap = t;
+  }
+  BCK(cudaMemcpyAsync(b->d_tiles, table.data(), t * sizeof(uint2), cudaMemcpyHostToDevice, b->stream),
+      "upload tile list");
   BCK(cudaMemcpyAsync(b->d_dom, b->h_dom.data(), b->h_dom.size() * sizeof(lbm::BatchDomain),
                       cudaMemcpyHostToDevice, b->stream),
       "upload tile table");

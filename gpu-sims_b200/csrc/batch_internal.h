@@ -8,6 +8,13 @@
 
 namespace lbm {
 
+// Whether batched domains may use the two-nodes-per-thread row update.  Off:
+// with both row updates in one kernel the batch ran slower on B200 (fp16
+// ensemble 20.3 vs 25.2 GLUPS), the domains being small.
+#ifndef LBM_BATCH_PAIRS
+#define LBM_BATCH_PAIRS 0
+#endif
+
 constexpr unsigned BATCH_STATUS_NONFINITE = 1u;  // same bit the single-domain step sets
 constexpr unsigned BATCH_STATUS_TIMEOUT = 2u;    // a grid-barrier wait gave up
 
@@ -27,6 +34,7 @@ static_assert(sizeof(BatchDomain) % 4 == 0, "copied as 32-bit words");
 
 struct BatchLaunch {
   BatchDomain* dom;       // device array [ndom]
+  const uint2* tiles;     // per tile: (domain, tile index within the domain)
   int ndom;
   uint32_t ntiles;
   int rows, nzt;          // block = 32 x rows threads; z-planes per thread

@@ -63,6 +63,9 @@ cudaError_t ref_step(const Ctx& c, const float* fin, float* fout, bool write_mom
 cudaError_t phys_init(const Ctx& c, const float* rho, const float* u3, float rho0,
                       const float* u0, cudaStream_t s);
 cudaError_t phys_step(const Ctx& c, int parity, bool write_moments, cudaStream_t s);
+cudaError_t phys_step_f32(const Ctx& c, int parity, bool write_moments, cudaStream_t s);
+cudaError_t phys_step_f16(const Ctx& c, int parity, bool write_moments, cudaStream_t s);
+cudaError_t phys_step_bf16(const Ctx& c, int parity, bool write_moments, cudaStream_t s);
 cudaError_t phys_read_pops(const Ctx& c, float* out, cudaStream_t s);
 cudaError_t phys_write_pops(const Ctx& c, const float* in, cudaStream_t s);
 

@@ -5,9 +5,9 @@
 // Work list.  Every domain is cut into tiles of 32 (64 when a thread takes two
 // nodes) x R x Z nodes (R rows per block, Z z-planes per thread, chosen by the
 // schedule/autotuner); tiles are
-// numbered domain after domain and a block finds its domain by binary search
-// over the first-tile table, then copies that domain's parameters into shared
-// memory.  The node update is the single-domain step_row / step_row2
+// numbered domain after domain; a table gives each tile's domain and its
+// index within the domain, and the block copies that domain's parameters
+// into shared memory.  The node update is the single-domain step_row / step_row2
 // (phys_step.cuh) chosen by the same rule, so a domain advanced in a batch is
 // bit-identical to the same domain advanced alone.
 //
@@ -24,19 +24,15 @@
 namespace lbm {
 namespace {
 
-__device__ __forceinline__ void load_tile(const BatchDomain* __restrict__ dp, int ndom, uint32_t t,
+__device__ __forceinline__ void load_tile(const BatchDomain* __restrict__ dp,
+                                          const uint2* __restrict__ tiles, uint32_t t,
                                           BatchDomain& sD, uint32_t& s_local) {
-  __shared__ int s_dom;
+  __shared__ uint32_t s_dom;
   const int tid = threadIdx.x + 32 * threadIdx.y;
   if (tid == 0) {
-    int lo = 0, hi = ndom - 1;  // last domain with tile_begin <= t
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (dp[mid].tile_begin <= t) lo = mid;
-      else hi = mid - 1;
-    }
-    s_dom = lo;
-    s_local = t - dp[lo].tile_begin;
+    const uint2 e = tiles[t];
+    s_dom = e.x;
+    s_local = e.y;
   }
   __syncthreads();
   const uint32_t* src = reinterpret_cast<const uint32_t*>(dp + s_dom);
@@ -58,7 +54,7 @@ __device__ __forceinline__ void batch_tile(const BatchDomain& D, uint32_t local,
   for (int k = 0; k < nzt; ++k) {
     const int z = tz * nzt + k;
     if (z >= D.p.g.nz) break;
-    if (D.pairs)  // uniform over the block
+    if (LBM_BATCH_PAIRS && D.pairs)  // uniform over the block
       step_row2<PREC, COLL, false, false, WM, P>(D.p, D.pop, D.flags, D.links, D.rho, D.u, status,
                                                  tx * 64, y, z);
     else
@@ -68,15 +64,16 @@ __device__ __forceinline__ void batch_tile(const BatchDomain& D, uint32_t local,
 }
 
 #ifndef LBM_BATCH_MINB
-#define LBM_BATCH_MINB 3
+#define LBM_BATCH_MINB 4
 #endif
 
 template <int PREC, int COLL, bool WM, int P>
 __global__ void __launch_bounds__(256, LBM_BATCH_MINB)
-    k_batch_step(const BatchDomain* __restrict__ dp, int ndom, int nzt, unsigned* status) {
+    k_batch_step(const BatchDomain* __restrict__ dp, const uint2* __restrict__ tiles, int nzt,
+                 unsigned* status) {
   __shared__ BatchDomain sD;
   __shared__ uint32_t s_local;
-  load_tile(dp, ndom, blockIdx.x, sD, s_local);
+  load_tile(dp, tiles, blockIdx.x, sD, s_local);
   batch_tile<PREC, COLL, WM, P>(sD, s_local, nzt, status);
 }
 
@@ -117,7 +114,8 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned expected, l
 
 template <int PREC, int COLL>
 __global__ void __launch_bounds__(256, LBM_BATCH_MINB)
-    k_batch_persistent(const BatchDomain* __restrict__ dp, int ndom, uint32_t ntiles, int nzt,
+    k_batch_persistent(const BatchDomain* __restrict__ dp, const uint2* __restrict__ tiles,
+                       uint32_t ntiles, int nzt,
                        int nsteps, int P0, unsigned* bar, unsigned expected, long long spin,
                        unsigned* status) {
   __shared__ BatchDomain sD;
@@ -126,7 +124,7 @@ __global__ void __launch_bounds__(256, LBM_BATCH_MINB)
     const int P = (P0 + st) & 1;
     const bool wm = st == nsteps - 1;
     for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-      load_tile(dp, ndom, t, sD, s_local);
+      load_tile(dp, tiles, t, sD, s_local);
       if (P) {
         if (wm) batch_tile<PREC, COLL, true, 1>(sD, s_local, nzt, status);
         else batch_tile<PREC, COLL, false, 1>(sD, s_local, nzt, status);
@@ -144,7 +142,7 @@ template <int PREC, int COLL>
 cudaError_t step_launch(const BatchLaunch& L, int P, bool wm, cudaStream_t s) {
   const dim3 blk(32, L.rows, 1);
 #define LBM_BATCH_LAUNCH(WM, PAR) \
-  k_batch_step<PREC, COLL, WM, PAR><<<L.ntiles, blk, 0, s>>>(L.dom, L.ndom, L.nzt, L.status)
+  k_batch_step<PREC, COLL, WM, PAR><<<L.ntiles, blk, 0, s>>>(L.dom, L.tiles, L.nzt, L.status)
   if (wm) {
     if (P) LBM_BATCH_LAUNCH(true, 1); else LBM_BATCH_LAUNCH(true, 0);
   } else {
@@ -196,11 +194,12 @@ cudaError_t batch_persistent(const BatchLaunch& L, int nsteps, int P0, int grid,
   const unsigned expected = (unsigned)grid + (unsigned)L.missing_blocks;
   long long spin = L.spin_limit;
   BatchDomain* dom = L.dom;
-  int ndom = L.ndom, nzt = L.nzt;
+  const uint2* tiles = L.tiles;
+  int nzt = L.nzt;
   uint32_t ntiles = L.ntiles;
   unsigned* bar = L.bar;
   unsigned* status = L.status;
-  void* args[] = {&dom, &ndom, &ntiles, &nzt, &nsteps, &P0, &bar, (void*)&expected, &spin, &status};
+  void* args[] = {&dom, (void*)&tiles, &ntiles, &nzt, &nsteps, &P0, &bar, (void*)&expected, &spin, &status};
   return cudaLaunchCooperativeKernel(pick_persistent(L.precision, L.collision), dim3(grid),
                                      dim3(32, L.rows, 1), args, 0, s);
 }
