@@ -287,6 +287,31 @@ int lbm_set_stream(lbm_ctx* c, void* stream) {
   return LBM_OK;
 }
 
+int lbm_set_closure(lbm_ctx* c, const float* net) {
+  if (int rc = check_ctx(c)) return rc;
+  if (c->d.mode != LBM_MODE_PHYSICS) return fail(c, LBM_ERR_UNSUPPORTED, "the closure needs physics mode");
+  if (net) {
+    if (!(c->d.smagorinsky_cs > 0.f))
+      return fail(c, LBM_ERR_INVALID_ARG, "the closure scales smagorinsky_cs, which must be > 0");
+    if (c->pp.accel[0] != 0.f || c->pp.accel[1] != 0.f || c->pp.accel[2] != 0.f)
+      return fail(c, LBM_ERR_UNSUPPORTED, "the closure kernels are built without a body force");
+    for (int k = 0; k < LBM_CLOSURE_FLOATS; ++k)
+      if (!std::isfinite(net[k])) return fail(c, LBM_ERR_INVALID_ARG, "closure network has a non-finite value");
+  }
+  // Captured step graphs hold the old network by value: rebuild them.
+  CK(cudaStreamSynchronize(c->stream), "set_closure sync");
+  for (auto& g : c->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  c->closure = net != nullptr;
+  for (int k = 0; k < LBM_CLOSURE_FLOATS; ++k) {
+    c->clo[k] = !net ? 0.f : lbm::clo_is_weight(k) ? lbm::round_bf16(net[k]) : net[k];
+  }
+  return LBM_OK;
+}
+
 int lbm_set_flags(lbm_ctx* c, const uint8_t* mask, size_t n) {
   if (int rc = check_ctx(c)) return rc;
   if (!mask) return fail(c, LBM_ERR_INVALID_ARG, "mask is NULL");

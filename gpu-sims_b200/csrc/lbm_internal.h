@@ -6,8 +6,32 @@
 #include <string>
 
 #include "../../include/lbm.h"
+#include "../../include/lbm_closure.h"
 
 namespace lbm {
+
+// Layout of a learned-closure network (lbm_closure.h).
+constexpr int CLO_IN = 9, CLO_HID = 32;
+// Parameter offsets in the packed float layout (also the gradient layout).
+constexpr int CLO_W1 = 0;                          // [32][9]
+constexpr int CLO_B1 = CLO_W1 + CLO_HID * CLO_IN;  // [32]
+constexpr int CLO_W2 = CLO_B1 + CLO_HID;           // [32][32]
+constexpr int CLO_B2 = CLO_W2 + CLO_HID * CLO_HID; // [32]
+constexpr int CLO_W3 = CLO_B2 + CLO_HID;           // [32]
+constexpr int CLO_B3 = CLO_W3 + CLO_HID;           // [1]
+constexpr int CLO_NPARAM = CLO_B3 + 1;             // 1409
+// A network: parameters (weights holding bf16 values), then the input mean
+// and inverse scale.
+constexpr int CLO_MEAN = CLO_NPARAM;
+constexpr int CLO_ISCALE = CLO_MEAN + CLO_IN;
+constexpr int CLO_FLOATS = CLO_ISCALE + CLO_IN;    // 1427
+
+constexpr bool clo_is_weight(int k) {
+  return (k >= CLO_W1 && k < CLO_B1) || (k >= CLO_W2 && k < CLO_B2) || (k >= CLO_W3 && k < CLO_B3);
+}
+
+static_assert(CLO_NPARAM == LBM_CLOSURE_PARAMS && CLO_FLOATS == LBM_CLOSURE_FLOATS,
+              "closure layout");
 
 // Launch-time parameters of the reference-mode (two-buffer) kernels.
 struct RefParams {
@@ -66,6 +90,9 @@ cudaError_t phys_step(const Ctx& c, int parity, bool write_moments, cudaStream_t
 cudaError_t phys_step_f32(const Ctx& c, int parity, bool write_moments, cudaStream_t s);
 cudaError_t phys_step_f16(const Ctx& c, int parity, bool write_moments, cudaStream_t s);
 cudaError_t phys_step_bf16(const Ctx& c, int parity, bool write_moments, cudaStream_t s);
+cudaError_t phys_step_clo_f32(const Ctx& c, int parity, bool write_moments, cudaStream_t s);
+cudaError_t phys_step_clo_f16(const Ctx& c, int parity, bool write_moments, cudaStream_t s);
+cudaError_t phys_step_clo_bf16(const Ctx& c, int parity, bool write_moments, cudaStream_t s);
 cudaError_t phys_read_pops(const Ctx& c, float* out, cudaStream_t s);
 cudaError_t phys_write_pops(const Ctx& c, const float* in, cudaStream_t s);
 
@@ -106,6 +133,10 @@ struct Ctx {
   // starting parity (reference mode: per current buffer), built on first use.
   static constexpr int kGraphSteps = 16;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  // learned closure (lbm_set_closure): the network the step kernels take by
+  // value; weights already rounded to bf16
+  bool closure = false;
+  float clo[LBM_CLOSURE_FLOATS] = {};
   bool initialized = false;
   uint64_t iteration = 0;
   uint64_t dev_bytes = 0;
@@ -113,6 +144,9 @@ struct Ctx {
 };
 
 size_t elem_bytes(int precision);
+// bfloat16 rounding, nearest even (NaN kept), of one float: the weights of a
+// closure network as the kernels use them.
+float round_bf16(float v);
 // Fills c.pp (padded geometry and physics parameters) from a physics-mode
 // descriptor; false if a slot array would exceed 2^32 elements.
 bool setup_physics(Ctx& c, const lbm_desc& d);

@@ -55,11 +55,11 @@ __device__ __forceinline__ void batch_tile(const BatchDomain& D, uint32_t local,
     const int z = tz * nzt + k;
     if (z >= D.p.g.nz) break;
     if (LBM_BATCH_PAIRS && D.pairs)  // uniform over the block
-      step_row2<PREC, COLL, false, false, WM, P>(D.p, D.pop, D.flags, D.links, D.rho, D.u, status,
-                                                 tx * 64, y, z);
+      step_row2<PREC, COLL, 0, false, WM, P>(D.p, CloNet<0>{}, D.pop, D.flags, D.links, D.rho, D.u,
+                                             status, tx * 64, y, z);
     else
-      step_row<PREC, COLL, false, false, WM, P>(D.p, D.pop, D.flags, D.links, D.rho, D.u, status,
-                                                tx * 32, y, z);
+      step_row<PREC, COLL, 0, false, WM, P>(D.p, CloNet<0>{}, D.pop, D.flags, D.links, D.rho, D.u,
+                                            status, tx * 32, y, z);
   }
 }
 

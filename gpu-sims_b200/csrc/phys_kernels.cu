@@ -154,8 +154,16 @@ dim3 phys_grid(const PhysGeom& g) {
 bool step_pairs_host(int nx) { return step_pairs(nx); }
 
 // The step kernels of each storage precision are compiled in their own
-// translation unit (phys_step_f32.cu, phys_step_f16.cu, phys_step_bf16.cu).
+// translation unit (phys_step_f32.cu, phys_step_f16.cu, phys_step_bf16.cu),
+// and so are their learned-closure variants (phys_step_clo_*.cu).
 cudaError_t phys_step(const Ctx& c, int parity, bool write_moments, cudaStream_t s) {
+  if (c.closure) {
+    switch (c.d.precision) {
+      case LBM_PREC_F32: return phys_step_clo_f32(c, parity, write_moments, s);
+      case LBM_PREC_F16S: return phys_step_clo_f16(c, parity, write_moments, s);
+      default: return phys_step_clo_bf16(c, parity, write_moments, s);
+    }
+  }
   switch (c.d.precision) {
     case LBM_PREC_F32: return phys_step_f32(c, parity, write_moments, s);
     case LBM_PREC_F16S: return phys_step_f16(c, parity, write_moments, s);

@@ -7,6 +7,8 @@
 #include <cuda_fp16.h>
 
 #include "d3q19.cuh"
+#include "closure.cuh"
+#include "fops.cuh"
 #include "lbm_internal.h"
 
 namespace lbm {
@@ -82,36 +84,6 @@ __device__ __forceinline__ float wall_term(const PhysParams& p, int x, int y, in
   return 6.0f * wf(J) * cu;
 }
 
-// Arithmetic policies for the collision.  Every operation is an explicitly
-// rounded intrinsic (no compiler contraction), so the one-node policy and
-// the two-node policy built on Blackwell's packed fp32 instructions
-// (FADD2/FMUL2/FFMA2: one instruction for two lanes' values) evaluate the
-// same operation graph and give bit-identical populations.
-struct Ops1 {
-  using F = float;
-  static __device__ __forceinline__ F splat(float c) { return c; }
-  static __device__ __forceinline__ F add(F a, F b) { return __fadd_rn(a, b); }
-  static __device__ __forceinline__ F sub(F a, F b) { return __fsub_rn(a, b); }
-  static __device__ __forceinline__ F mul(F a, F b) { return __fmul_rn(a, b); }
-  static __device__ __forceinline__ F fma(F a, F b, F c) { return __fmaf_rn(a, b, c); }
-  static __device__ __forceinline__ F div(F a, F b) { return __fdiv_rn(a, b); }
-  static __device__ __forceinline__ F sqrt(F a) { return __fsqrt_rn(a); }
-};
-struct Ops2 {
-  using F = float2;
-  static __device__ __forceinline__ F splat(float c) { return make_float2(c, c); }
-  static __device__ __forceinline__ F add(F a, F b) { return __fadd2_rn(a, b); }
-  // a - b as b * (-1) + a: the product is exact, so the single rounding
-  // equals that of a - b.
-  static __device__ __forceinline__ F sub(F a, F b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
-  static __device__ __forceinline__ F mul(F a, F b) { return __fmul2_rn(a, b); }
-  static __device__ __forceinline__ F fma(F a, F b, F c) { return __ffma2_rn(a, b, c); }
-  static __device__ __forceinline__ F div(F a, F b) {
-    return make_float2(__fdiv_rn(a.x, b.x), __fdiv_rn(a.y, b.y));
-  }
-  static __device__ __forceinline__ F sqrt(F a) { return make_float2(__fsqrt_rn(a.x), __fsqrt_rn(a.y)); }
-};
-
 // Collision on shifted populations in storage units v = SC (f - w), in
 // place, written per opposite pair (a, b): with cu = c_a . u the equilibrium
 // splits into an even part  w (drho + rho (4.5 cu^2 - 1.5 u.u))  shared by a
@@ -124,8 +96,9 @@ struct Ops2 {
 // (1 - omega/2) even source, O = omega- odd + (1 - omega-/2) odd source.
 // Returns rho and the force-shifted velocity u = (sum c f + F/2) / rho.
 // O is Ops1 (one node) or Ops2 (two nodes in the .x/.y lanes).
-template <class O, int COLL, bool SMAG, bool FORCE, int PREC>
-__device__ __forceinline__ void collide_t(const PhysParams& p, typename O::F (&g)[Q],
+template <class O, int COLL, int SGS, bool FORCE, int PREC>
+__device__ __forceinline__ void collide_t(const PhysParams& p, const CloNet<SGS>& net,
+                                          typename O::F (&g)[Q],
                                           typename O::F& rho_out, typename O::F& ux,
                                           typename O::F& uy, typename O::F& uz) {
   using F = typename O::F;
@@ -157,7 +130,7 @@ __device__ __forceinline__ void collide_t(const PhysParams& p, typename O::F (&g
   const F sr = O::mul(O::splat(SC), rho);
 
   F omega = O::splat(p.omega);
-  if (SMAG) {
+  if (SGS) {
     // Pi = sum c c (f - feq) (even in c: pair sums suffice); Hou et al. (1996)
     //   tau_eff = (tau + sqrt(tau^2 + 18 sqrt(2) Cs^2 |Pi| / rho)) / 2.
     F pxx = O::splat(0.f), pyy = pxx, pzz = pxx, pxy = pxx, pxz = pxx, pyz = pxx;
@@ -187,8 +160,17 @@ __device__ __forceinline__ void collide_t(const PhysParams& p, typename O::F (&g
     const F q = O::fma(pxx, pxx, O::fma(pyy, pyy, O::fma(pzz, pzz, O::mul(O::splat(2.f), off))));
     const F pn = O::mul(O::splat(INV), O::sqrt(q));
     const float cs2 = p.smag_cs * p.smag_cs;
-    const F arg = O::fma(O::splat(p.tau), O::splat(p.tau),
-                         O::div(O::mul(O::splat(25.455844f * cs2), pn), rho));
+    F k2 = O::splat(25.455844f * cs2);
+    if (SGS == 2) {
+      // learned closure: Cs^2 = Cs0^2 r(features of Pi, rho)
+      const F P[6] = {O::mul(O::splat(INV), pxx), O::mul(O::splat(INV), pyy),
+                      O::mul(O::splat(INV), pzz), O::mul(O::splat(INV), pxy),
+                      O::mul(O::splat(INV), pxz), O::mul(O::splat(INV), pyz)};
+      F xin[CLO_IN];
+      closure_features<O>(P, rho, xin);
+      k2 = O::mul(k2, closure_mlp<O>(net, xin));
+    }
+    const F arg = O::fma(O::splat(p.tau), O::splat(p.tau), O::div(O::mul(k2, pn), rho));
     const F tau_eff = O::mul(O::splat(0.5f), O::add(O::splat(p.tau), O::sqrt(arg)));
     omega = O::div(O::splat(1.0f), tau_eff);
   }
@@ -255,10 +237,10 @@ __device__ __forceinline__ void collide_t(const PhysParams& p, typename O::F (&g
   });
 }
 
-template <int COLL, bool SMAG, bool FORCE, int PREC>
-__device__ __forceinline__ void collide(const PhysParams& p, float (&g)[Q], float& rho_out,
-                                        float& ux, float& uy, float& uz) {
-  collide_t<Ops1, COLL, SMAG, FORCE, PREC>(p, g, rho_out, ux, uy, uz);
+template <int COLL, int SGS, bool FORCE, int PREC>
+__device__ __forceinline__ void collide(const PhysParams& p, const CloNet<SGS>& net, float (&g)[Q],
+                                        float& rho_out, float& ux, float& uy, float& uz) {
+  collide_t<Ops1, COLL, SGS, FORCE, PREC>(p, net, g, rho_out, ux, uy, uz);
 }
 
 // Launch shape of the step kernel: a block is 32 x STEP_BY nodes of one
@@ -325,8 +307,9 @@ __device__ __forceinline__ uint32_t offs(const PhysGeom& G, const Wrap& w) {
 // One warp updates nodes x0 .. x0+31 of row (y, z); y < ny (the caller's
 // test is uniform over the warp).  Used by the single-domain kernel and by
 // the batched kernels (phys_batch.cu).
-template <int PREC, int COLL, bool SMAG, bool FORCE, bool WRITE_MOMENTS, int P>
-__device__ __forceinline__ void step_row(const PhysParams& p, void* __restrict__ pop_v,
+template <int PREC, int COLL, int SGS, bool FORCE, bool WRITE_MOMENTS, int P>
+__device__ __forceinline__ void step_row(const PhysParams& p, const CloNet<SGS>& net,
+                                         void* __restrict__ pop_v,
                                          const uint8_t* __restrict__ flags,
                                          const uint32_t* __restrict__ links,
                                          float* __restrict__ rho_o, float* __restrict__ u_o,
@@ -420,7 +403,7 @@ __device__ __forceinline__ void step_row(const PhysParams& p, void* __restrict__
   }
 
   float rho, ux, uy, uz;
-  collide<COLL, SMAG, FORCE, PREC>(p, g, rho, ux, uy, uz);
+  collide<COLL, SGS, FORCE, PREC>(p, net, g, rho, ux, uy, uz);
 
   if (WRITE_MOMENTS && valid) {
     const bool s = !fluid;
@@ -509,8 +492,9 @@ template <> struct Vec2<LBM_PREC_BF16S> {
 // packed fp32 instructions (Ops2).  Solid nodes are never written (their
 // slots hold neighbours' bounce-back values), so a pair with a solid node
 // stores element-wise.
-template <int PREC, int COLL, bool SMAG, bool FORCE, bool WRITE_MOMENTS, int P>
-__device__ __forceinline__ void step_row2(const PhysParams& p, void* __restrict__ pop_v,
+template <int PREC, int COLL, int SGS, bool FORCE, bool WRITE_MOMENTS, int P>
+__device__ __forceinline__ void step_row2(const PhysParams& p, const CloNet<SGS>& net,
+                                          void* __restrict__ pop_v,
                                           const uint8_t* __restrict__ flags,
                                           const uint32_t* __restrict__ links,
                                           float* __restrict__ rho_o, float* __restrict__ u_o,
@@ -606,7 +590,7 @@ __device__ __forceinline__ void step_row2(const PhysParams& p, void* __restrict_
   if (fluidB && (flB & FLAG_SOLID_LINK)) solid_fix(IC<1>{}, nid + 1, lnB, wB, false, xhiB);
 
   float2 r2, ux2, uy2, uz2;
-  collide_t<Ops2, COLL, SMAG, FORCE, PREC>(p, g2, r2, ux2, uy2, uz2);
+  collide_t<Ops2, COLL, SGS, FORCE, PREC>(p, net, g2, r2, ux2, uy2, uz2);
 
   if (WRITE_MOMENTS && valid) {
     *reinterpret_cast<float2*>(rho_o + nid) = make_float2(fluidA ? r2.x : 0.f, fluidB ? r2.y : 0.f);

@@ -1,0 +1,4 @@
+// Physics-mode step kernels with the learned closure, f16 population storage.
+#include "phys_step_launch.cuh"
+
+LBM_DEFINE_PHYS_STEP(phys_step_clo_f16, LBM_PREC_F16S, true)

@@ -89,8 +89,23 @@ class BatchInfo(C.Structure):
     ]
 
 
-# Every symbol include/lbm.h declares, with its ctypes signature.
+class Adam(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_uint32), ("lr", C.c_float), ("beta1", C.c_float),
+        ("beta2", C.c_float), ("eps", C.c_float), ("weight_decay", C.c_float),
+    ]
+
+
+# include/lbm_closure.h
+CLOSURE_INPUTS = 9
+CLOSURE_HIDDEN = 32
+CLOSURE_PARAMS = 1409
+CLOSURE_FLOATS = 1427
+
+# Every symbol include/lbm.h and include/lbm_closure.h declare, with its
+# ctypes signature.
 _P = C.c_void_p
+_I32, _I64, _U64, _F = C.c_int32, C.c_int64, C.c_uint64, C.c_float
 _SIGS = {
     "lbm_desc_default": (C.c_int, [C.POINTER(Desc)]),
     "lbm_create": (C.c_int, [C.POINTER(Desc), C.POINTER(_P)]),
@@ -131,6 +146,20 @@ _SIGS = {
     "lbm_batch_autotune": (C.c_int, [_P, C.c_int, C.POINTER(BatchSchedule)]),
     "lbm_batch_get_info": (C.c_int, [_P, C.POINTER(BatchInfo)]),
     "lbm_batch_last_error": (C.c_char_p, [_P]),
+    "lbm_set_closure": (C.c_int, [_P, _P]),
+    "lbm_box_filter": (C.c_int, [_P, _P, _I32, _I32, _I32, _I32, _P, _P]),
+    "lbm_closure_samples": (C.c_int, [_P, _I32, _I32, _I32, _F, _F, _U64, _I64, _P, _P, _P, _P]),
+    "lbm_closure_predict": (C.c_int, [_P, _P, _I64, _P, _P]),
+    "lbm_adam_default": (C.c_int, [C.POINTER(Adam)]),
+    "lbm_trainer_create": (C.c_int, [_P, C.POINTER(Adam), C.POINTER(_P)]),
+    "lbm_trainer_destroy": (C.c_int, [_P]),
+    "lbm_trainer_set_stream": (C.c_int, [_P, _P]),
+    "lbm_trainer_grad": (C.c_int, [_P, _P, _P, _P, _I64, _F, _P, C.POINTER(C.c_double)]),
+    "lbm_trainer_adam_step": (C.c_int, [_P]),
+    "lbm_trainer_fit": (C.c_int, [_P, _P, _P, _P, _I64, _I32, _I32, _U64, _P]),
+    "lbm_trainer_get_net": (C.c_int, [_P, _P]),
+    "lbm_trainer_last_error": (C.c_char_p, [_P]),
+    "lbm_round_bf16": (C.c_int, [_P, _P, C.c_size_t]),
 }
 
 _lib = None
@@ -247,6 +276,17 @@ class Lattice:
     def set_flags(self, mask: np.ndarray) -> None:
         m = np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
         self._c(load().lbm_set_flags(self._h, _ptr(m), m.size))
+
+    def set_closure(self, net: np.ndarray | None) -> None:
+        """Installs a learned-closure network (float[CLOSURE_FLOATS]); None
+        removes it."""
+        if net is None:
+            self._c(load().lbm_set_closure(self._h, None))
+            return
+        w = np.ascontiguousarray(net, dtype=np.float32).reshape(-1)
+        if w.size != CLOSURE_FLOATS:
+            raise LbmError(ERR_INVALID_ARG, f"network must have {CLOSURE_FLOATS} floats")
+        self._c(load().lbm_set_closure(self._h, _ptr(w)))
 
     def read_classification(self) -> np.ndarray:
         out = np.zeros(self.n, np.uint32)
@@ -448,3 +488,95 @@ def apply_preset(lat: Lattice, preset_idx: int) -> np.ndarray:
     lat.set_flags(mask)
     lat.init_equilibrium(1.0, tuple(lat.desc.u_inf))
     return mask
+
+
+# ---- learned closure (include/lbm_closure.h) --------------------------------
+# Device arguments are raw device pointers (ints), e.g. torch's data_ptr();
+# `stream` is a cudaStream_t handle or None.
+
+def round_bf16(a: np.ndarray) -> np.ndarray:
+    x = np.ascontiguousarray(a, dtype=np.float32)
+    out = np.empty_like(x)
+    _check(load().lbm_round_bf16(_ptr(x), _ptr(out), x.size))
+    return out
+
+
+def box_filter(d_rho: int, d_u: int, shape, factor: int, d_out: int, stream=None) -> None:
+    nx, ny, nz = shape
+    _check(load().lbm_box_filter(d_rho, d_u, nx, ny, nz, factor, d_out, stream))
+
+
+def closure_samples(d_filt: int, shape, tau: float, cs0: float, seed: int, n_samples: int,
+                    d_x: int, d_target: int, d_weight: int, stream=None) -> None:
+    nx, ny, nz = shape
+    _check(load().lbm_closure_samples(d_filt, nx, ny, nz, tau, cs0, seed, n_samples,
+                                      d_x, d_target, d_weight, stream))
+
+
+def closure_predict(net: np.ndarray, d_x: int, n: int, d_r: int, stream=None) -> None:
+    w = np.ascontiguousarray(net, dtype=np.float32).reshape(-1)
+    if w.size != CLOSURE_FLOATS:
+        raise LbmError(ERR_INVALID_ARG, f"network must have {CLOSURE_FLOATS} floats")
+    _check(load().lbm_closure_predict(_ptr(w), d_x, n, d_r, stream))
+
+
+def adam_default(**kw) -> Adam:
+    a = Adam()
+    _check(load().lbm_adam_default(C.byref(a)))
+    for k, v in kw.items():
+        setattr(a, k, v)
+    return a
+
+
+class Trainer:
+    """Fused forward/backward + Adam training of a closure network on the
+    current CUDA device (lbm_trainer_*)."""
+
+    def __init__(self, net: np.ndarray, adam: Adam | None = None):
+        w = np.ascontiguousarray(net, dtype=np.float32).reshape(-1)
+        if w.size != CLOSURE_FLOATS:
+            raise LbmError(ERR_INVALID_ARG, f"network must have {CLOSURE_FLOATS} floats")
+        self.adam = adam if adam is not None else adam_default()
+        h = _P()
+        _check(load().lbm_trainer_create(_ptr(w), C.byref(self.adam), C.byref(h)))
+        self._h = h
+
+    def _c(self, rc: int) -> None:
+        if rc != OK:
+            raise LbmError(rc, load().lbm_trainer_last_error(self._h).decode())
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            load().lbm_trainer_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream) -> None:
+        self._c(load().lbm_trainer_set_stream(self._h, stream))
+
+    def grad(self, d_x: int, d_target: int, d_weight: int, n: int, wscale: float):
+        g = np.empty(CLOSURE_PARAMS, np.float32)
+        loss = C.c_double()
+        self._c(load().lbm_trainer_grad(self._h, d_x, d_target, d_weight, n, wscale, _ptr(g),
+                                        C.byref(loss)))
+        return g, loss.value
+
+    def adam_step(self) -> None:
+        self._c(load().lbm_trainer_adam_step(self._h))
+
+    def fit(self, d_x: int, d_target: int, d_weight: int, n: int, batch: int, epochs: int,
+            seed: int = 1) -> np.ndarray:
+        losses = np.zeros(max(epochs, 1), np.float64)
+        self._c(load().lbm_trainer_fit(self._h, d_x, d_target, d_weight, n, batch, epochs, seed,
+                                       _ptr(losses)))
+        return losses[:epochs]
+
+    def net(self) -> np.ndarray:
+        out = np.empty(CLOSURE_FLOATS, np.float32)
+        self._c(load().lbm_trainer_get_net(self._h, _ptr(out)))
+        return out

@@ -5,7 +5,8 @@
 // periodic wrap or half-way bounce-back, momentum-corrected moving walls
 // (f_i = f*_opp(i) + 6 w_i rho_w (c_i . u_w), rho_w = 1; a link leaving the
 // box through a z face takes that face's velocity, then y, then x), BGK or
-// TRT, Smagorinsky (Hou et al. 1996) and Guo forcing with F = rho g.  Both
+// TRT, Smagorinsky (Hou et al. 1996), optionally with the learned closure
+// (Cs^2 scaled per node by a network), and Guo forcing with F = rho g.  Both
 // builds round every operation on its own (-ffp-contract=off / -fmad=false)
 // in the same order, so CPU and GPU FP64 results agree bit for bit.
 #pragma once
@@ -62,6 +63,10 @@ template <class T> OX_HD inline T feq_i(int i, T rho, T ux, T uy, T uz) {
   return weight<T>(i) * rho * (T(1) + T(3) * cdotu + T(4.5) * cdotu * cdotu - T(1.5) * udotu);
 }
 
+// Learned-closure network, layout of include/lbm_closure.h: W1[32][9] b1[32]
+// W2[32][32] b2[32] W3[32] b3, input mean[9], input inverse scale[9].
+constexpr int NET_FLOATS = 1427;
+
 struct ExtP {
   int nx, ny, nz;
   int periodic[3];
@@ -71,9 +76,12 @@ struct ExtP {
   double smag_cs;
   double accel[3];
   double wall[6][3];
+  int has_net;    // learned closure: Cs^2 = smag_cs^2 * r(Pi, rho)
+  double net[NET_FLOATS];
 };
 
-// ip: nx ny nz px py pz collision; dp: tau trt_magic smag_cs accel[3] wall[18]
+// ip: nx ny nz px py pz collision;
+// dp: tau trt_magic smag_cs accel[3] wall[18] has_net [net[NET_FLOATS] if has_net]
 inline ExtP make_ext(const int* ip, const double* dp) {
   ExtP p;
   p.nx = ip[0]; p.ny = ip[1]; p.nz = ip[2];
@@ -83,7 +91,40 @@ inline ExtP make_ext(const int* ip, const double* dp) {
   for (int a = 0; a < 3; ++a) p.accel[a] = dp[3 + a];
   for (int f = 0; f < 6; ++f)
     for (int a = 0; a < 3; ++a) p.wall[f][a] = dp[6 + 3 * f + a];
+  p.has_net = dp[24] != 0.0;
+  for (int k = 0; k < NET_FLOATS; ++k) p.net[k] = p.has_net ? dp[25 + k] : 0.0;
   return p;
+}
+
+// Network output r for the flux P (xx yy zz xy xz yz) and density rho.
+template <class T>
+OX_HD inline T ext_closure_r(const ExtP& p, const T P[6], T rho) {
+  const double* w = p.net;
+  const T n = std::sqrt(P[0] * P[0] + P[1] * P[1] + P[2] * P[2] +
+                        T(2) * (P[3] * P[3] + P[4] * P[4] + P[5] * P[5])) + T(1e-30);
+  T q[6];
+  for (int k = 0; k < 6; ++k) q[k] = P[k] / n;
+  // tr(M^3) with M = [[xx,xy,xz],[xy,yy,yz],[xz,yz,zz]] by explicit products
+  const T M[3][3] = {{q[0], q[3], q[4]}, {q[3], q[1], q[5]}, {q[4], q[5], q[2]}};
+  T t3 = 0;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j)
+      for (int k = 0; k < 3; ++k) t3 += M[i][j] * M[j][k] * M[k][i];
+  T x[9] = {q[0], q[1], q[2], q[3], q[4], q[5], std::log(n), t3, rho - T(1)};
+  for (int j = 0; j < 9; ++j) x[j] = (x[j] - T(w[1409 + j])) * T(w[1418 + j]);
+  T h1[32];
+  for (int i = 0; i < 32; ++i) {
+    T a = T(w[288 + i]);
+    for (int j = 0; j < 9; ++j) a += T(w[i * 9 + j]) * x[j];
+    h1[i] = a > T(0) ? a : T(0);
+  }
+  T z = T(w[1408]);
+  for (int i = 0; i < 32; ++i) {
+    T a = T(w[1344 + i]);
+    for (int j = 0; j < 32; ++j) a += T(w[320 + i * 32 + j]) * h1[j];
+    z += T(w[1376 + i]) * (a > T(0) ? a : T(0));
+  }
+  return z > T(20) ? z : std::log(T(1) + std::exp(z));
 }
 
 OX_HD inline size_t nidx(int nx, int ny, int x, int y, int z) {
@@ -137,7 +178,11 @@ OX_HD inline void ext_collide_node(const ExtP& p, T* v, T& rho_o, T& ux_o, T& uy
     T q = 0;
     for (int a = 0; a < 3; ++a)
       for (int b = 0; b < 3; ++b) q += P[a][b] * P[a][b];
-    const T cs2 = T(p.smag_cs * p.smag_cs);
+    T cs2 = T(p.smag_cs * p.smag_cs);
+    if (p.has_net) {
+      const T Pv[6] = {P[0][0], P[1][1], P[2][2], P[0][1], P[0][2], P[1][2]};
+      cs2 = cs2 * ext_closure_r<T>(p, Pv, rho);
+    }
     tau = (tau + std::sqrt(tau * tau + T(18) * std::sqrt(T(2)) * cs2 * std::sqrt(q) / rho)) / T(2);
   }
   const T om = T(1) / tau;

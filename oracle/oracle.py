@@ -143,19 +143,32 @@ class RefState:
         return out
 
 
+def _ext_dp(tau, trt_magic, smag_cs, accel, wall, net):
+    """Double parameters of ExtStep (ext_step.h make_ext): tau, Lambda, Cs,
+    accel[3], wall[6][3], has_net, then the network (its weights as the
+    kernels use them, rounded to bf16) if one is given."""
+    parts = [[tau, trt_magic, smag_cs], np.asarray(accel, np.float64), np.asarray(wall, np.float64).reshape(-1)]
+    if net is None:
+        parts.append([0.0])
+    else:
+        from .closure_oracle import kernel_net
+        parts += [[1.0], kernel_net(net).astype(np.float64)]
+    return np.ascontiguousarray(np.concatenate(parts), np.float64)
+
+
 class ExtState:
     """Textbook stream-collide state: post-collision populations float[19][N]."""
 
     def __init__(self, shape, periodic=(0, 0, 0), tau=0.6, collision=0, trt_magic=3.0 / 16.0,
-                 smag_cs=0.0, accel=(0.0, 0.0, 0.0), wall=None, mask=None, dtype=np.float64):
+                 smag_cs=0.0, accel=(0.0, 0.0, 0.0), wall=None, mask=None, dtype=np.float64,
+                 net=None):
         self.shape = tuple(shape)
         nx, ny, nz = self.shape
         self.n = nx * ny * nz
         self.dtype = np.dtype(dtype)
         self.ip = np.array([nx, ny, nz, *periodic, collision], np.int32)
         w = np.zeros((6, 3)) if wall is None else np.asarray(wall, np.float64).reshape(6, 3)
-        self.dp = np.concatenate([[tau, trt_magic, smag_cs], np.asarray(accel, np.float64), w.reshape(-1)])
-        self.dp = np.ascontiguousarray(self.dp, np.float64)
+        self.dp = _ext_dp(tau, trt_magic, smag_cs, accel, w, net)
         self.mask = np.zeros(self.n, np.uint8) if mask is None else np.ascontiguousarray(mask, np.uint8).reshape(-1)
         self.f = np.zeros((19, self.n), self.dtype)
         self.rho = np.zeros(self.n, self.dtype)
@@ -197,7 +210,7 @@ class ExtStateGPU:
     bit for bit); device memory through torch.  For full-size FP64 runs."""
 
     def __init__(self, shape, periodic=(0, 0, 0), tau=0.6, collision=0, trt_magic=3.0 / 16.0,
-                 smag_cs=0.0, accel=(0.0, 0.0, 0.0), wall=None, mask=None):
+                 smag_cs=0.0, accel=(0.0, 0.0, 0.0), wall=None, mask=None, net=None):
         import torch
         self.torch = torch
         self.shape = tuple(shape)
@@ -205,8 +218,7 @@ class ExtStateGPU:
         self.n = nx * ny * nz
         self.ip = np.array([nx, ny, nz, *periodic, collision], np.int32)
         w = np.zeros((6, 3)) if wall is None else np.asarray(wall, np.float64).reshape(6, 3)
-        self.dp = np.ascontiguousarray(np.concatenate([[tau, trt_magic, smag_cs],
-                                                       np.asarray(accel, np.float64), w.reshape(-1)]))
+        self.dp = _ext_dp(tau, trt_magic, smag_cs, accel, w, net)
         m = np.zeros(self.n, np.uint8) if mask is None else np.ascontiguousarray(mask, np.uint8).reshape(-1)
         dev = torch.device("cuda")
         self.mask = torch.from_numpy(m).to(dev)

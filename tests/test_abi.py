@@ -11,14 +11,15 @@ from conftest import ROOT, cuda_available
 
 
 def header_symbols():
-    text = (ROOT / "include" / "lbm.h").read_text()
+    text = "".join(h.read_text() for h in sorted((ROOT / "include").glob("*.h")))
     return sorted(set(re.findall(r"LBM_API\s+[\w\s\*]+?\b(lbm_\w+)\s*\(", text)))
 
 
 def test_library_exports_every_declared_symbol(lbm_lib):
     lib = C.CDLL(str(lbm_lib.LIB_PATH))
     syms = header_symbols()
-    assert len(syms) >= 20
+    assert len(syms) >= 50
+    assert "lbm_trainer_fit" in syms and "lbm_set_closure" in syms
     missing = [s for s in syms if not hasattr(lib, s)]
     assert not missing, missing
     # the Python layer binds every symbol too
@@ -94,3 +95,38 @@ def test_voxeliser_matches_oracle(lbm_lib, oracle, preset, shape):
 def test_voxeliser_rejects_bad_input(lbm_lib):
     with pytest.raises(lbm_lib.LbmError):
         lbm_lib.voxelize_naca("00x2", 8, 8, 1)
+
+
+def test_round_bf16_nearest_even(lbm_lib):
+    rng = np.random.default_rng(4)
+    x = np.concatenate([rng.standard_normal(20000).astype(np.float32) * 10.0 ** rng.integers(-30, 30, 20000),
+                        np.array([0.0, -0.0, 1.0, 3.4e38, -3.4e38, 1e-40, np.inf, -np.inf], np.float32)]).astype(np.float32)
+    got = lbm_lib.round_bf16(x)
+    # nearest-even on the upper 16 bits: the result is the closer of the two
+    # bf16 neighbours, and on a tie the one with an even last bit
+    b = x.view(np.uint32).astype(np.uint64)
+    lo = (b & 0xFFFF0000).astype(np.uint32).view(np.float32).astype(np.float64)
+    hi = ((b & 0xFFFF0000) + 0x10000).astype(np.uint32).view(np.float32).astype(np.float64)
+    finite = np.isfinite(x) & np.isfinite(hi)
+    xd = x.astype(np.float64)
+    dl, dh = np.abs(xd - lo), np.abs(hi - xd)
+    pick_hi = (dh < dl) | ((dh == dl) & (((b >> 16) & 1) == 1))
+    want = np.where(pick_hi, hi, lo)
+    assert np.array_equal(got[finite].astype(np.float64), want[finite])
+    assert np.array_equal(got[~np.isfinite(x)], x[~np.isfinite(x)])
+
+
+def test_closure_argument_checks_without_device(lbm_lib):
+    lib = lbm_lib.load()
+    assert lib.lbm_set_closure(None, None) == lbm_lib.ERR_INVALID_ARG
+    assert lib.lbm_box_filter(None, None, 8, 8, 8, 2, None, None) == lbm_lib.ERR_INVALID_ARG
+    assert lib.lbm_closure_predict(None, None, 1, None, None) == lbm_lib.ERR_INVALID_ARG
+    assert lib.lbm_trainer_create(None, None, None) == lbm_lib.ERR_INVALID_ARG
+    assert lib.lbm_trainer_destroy(None) == lbm_lib.OK
+    assert lib.lbm_trainer_fit(None, None, None, None, 1, 1, 1, 0, None) == lbm_lib.ERR_INVALID_ARG
+    assert lib.lbm_trainer_last_error(None)
+    a = lbm_lib.adam_default()
+    assert a.struct_size == C.sizeof(lbm_lib.Adam) and abs(a.lr - 1e-3) < 1e-9
+    # a factor that does not divide the grid is refused before any launch
+    p = C.c_void_p(16)
+    assert lib.lbm_box_filter(p, p, 9, 8, 8, 2, p, None) == lbm_lib.ERR_INVALID_ARG

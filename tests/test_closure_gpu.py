@@ -1,0 +1,293 @@
+"""Learned-closure kernels on the GPU against the FP64 numpy oracle
+(oracle/closure_oracle.py) and the FP64 ExtStep with the closure.
+
+Tolerances (written per test):
+  * box filter and training targets: fp64 sums of fp32 inputs rounded to
+    fp32 -> 1e-6 relative;
+  * features: fp32 evaluation -> 2e-6 absolute (inputs are O(1), log|Pi|
+    O(10));
+  * forward pass: fp32 accumulation over 1,344 products -> 1e-5 relative;
+  * gradient: fp32 sums over up to 40,000 samples -> 1e-4 of the largest
+    component, loss 1e-5 relative;
+  * fused step with the closure: as the physics-mode parity tests,
+    3e-5 of the velocity scale (fp32 storage).
+"""
+import numpy as np
+import pytest
+
+from oracle import closure_oracle as co
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+
+
+def _sync():
+    import torch
+    torch.cuda.synchronize()
+
+
+def _smooth_field(shape, seed, amp=0.04, kmax=3):
+    """Sum of a few random Fourier modes (periodic), u [3][n]."""
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = shape
+    z, y, x = np.meshgrid(np.arange(nz) / nz, np.arange(ny) / ny, np.arange(nx) / nx, indexing="ij")
+    u = np.zeros((3, nz, ny, nx))
+    for _ in range(6):
+        k = rng.integers(-kmax, kmax + 1, 3)
+        ph = rng.uniform(0, 2 * np.pi)
+        a = rng.standard_normal(3)
+        u += a[:, None, None, None] * np.sin(2 * np.pi * (k[0] * x + k[1] * y + k[2] * z) + ph)
+    u *= amp / np.sqrt((u ** 2).mean())
+    return u.reshape(3, -1)
+
+
+def _net(seed):
+    mean = np.array([0, 0, 0, 0, 0, 0, -6.0, 0, 0])
+    isc = np.array([1, 1, 1, 1, 1, 1, 0.5, 1, 50.0])
+    return co.random_net(seed, mean=mean, iscale=isc)
+
+
+@pytest.mark.parametrize("shape,f", [((16, 12, 8), 4), ((12, 8, 6), 2), ((6, 4, 2), 1)])
+def test_box_filter_matches_oracle(gpu, shape, f):
+    import torch
+    n = int(np.prod(shape))
+    rng = np.random.default_rng(n)
+    rho = (1 + 0.02 * rng.standard_normal(n)).astype(np.float32)
+    u = (0.04 * rng.standard_normal((3, n))).astype(np.float32)
+    nc = n // f ** 3
+    out = torch.empty(10 * nc, device="cuda")
+    d_rho, d_u = _dev(rho), _dev(u)  # held: a temporary's memory is reused at once
+    gpu.box_filter(d_rho.data_ptr(), d_u.data_ptr(), shape, f, out.data_ptr())
+    _sync()
+    got = out.cpu().numpy().reshape(10, nc)
+    want = co.box_filter(rho.astype(np.float64), u.astype(np.float64), shape, f)
+    assert np.allclose(got, want, rtol=1e-6, atol=1e-12)
+
+
+@pytest.mark.parametrize("seed,ns", [(0, None), (11, 777)])
+def test_samples_match_oracle(gpu, seed, ns):
+    import torch
+    shape = (16, 12, 10)
+    n = int(np.prod(shape))
+    rng = np.random.default_rng(3)
+    filt = np.zeros((10, n), np.float32)
+    filt[0] = 1 + 0.005 * rng.standard_normal(n)
+    filt[1:4] = _smooth_field(shape, 4)
+    filt[4:] = 2e-5 * rng.standard_normal((6, n))
+    ns = n if ns is None else ns
+    x = torch.empty(ns * 9, device="cuda")
+    t = torch.empty(ns, device="cuda")
+    w = torch.empty(ns, device="cuda")
+    d_filt = _dev(filt)
+    gpu.closure_samples(d_filt.data_ptr(), shape, 0.502, 0.1, seed, ns, x.data_ptr(),
+                        t.data_ptr(), w.data_ptr())
+    _sync()
+    xw, tw, ww = co.samples(filt.astype(np.float64), shape, 0.502, 0.1, seed, ns)
+    assert np.allclose(x.cpu().numpy().reshape(ns, 9), xw, rtol=0, atol=2e-6)
+    assert np.allclose(w.cpu().numpy(), ww, rtol=1e-6, atol=0)
+    assert np.allclose(t.cpu().numpy(), tw, rtol=1e-6, atol=1e-6 * np.abs(tw).max())
+
+
+def test_predict_matches_oracle(gpu):
+    import torch
+    rng = np.random.default_rng(6)
+    X = rng.standard_normal((5000, 9)).astype(np.float32)
+    X[:, 6] = -6 + 2 * X[:, 6]
+    net = _net(1)
+    r = torch.empty(5000, device="cuda")
+    dX = _dev(X)
+    gpu.closure_predict(net, dX.data_ptr(), 5000, r.data_ptr())
+    _sync()
+    want, _ = co.forward(co.kernel_net(net), X.astype(np.float64))
+    assert np.allclose(r.cpu().numpy(), want, rtol=1e-5, atol=1e-6)
+
+
+@pytest.mark.parametrize("n", [1000, 40000])
+def test_gradient_matches_fp64_oracle(gpu, n):
+    """The fused forward/backward kernel's gradient equals the FP64 oracle's
+    reverse-mode gradient at the same (bf16-rounded) weights."""
+    rng = np.random.default_rng(n)
+    X = rng.standard_normal((n, 9)).astype(np.float32)
+    X[:, 6] = -6 + 2 * X[:, 6]
+    t = rng.uniform(0, 3, n).astype(np.float32)
+    w = rng.uniform(0.1, 2, n).astype(np.float32)
+    net = _net(2)
+    tr = gpu.Trainer(net)
+    wscale = float(1.0 / w.astype(np.float64).sum())
+    dX, dt, dw = _dev(X), _dev(t), _dev(w)
+    g, loss = tr.grad(dX.data_ptr(), dt.data_ptr(), dw.data_ptr(), n, wscale)
+    L, gw = co.loss_and_grad(co.kernel_net(net), X.astype(np.float64), t, w, np.float32(wscale))
+    assert abs(loss - L) <= 1e-5 * L
+    assert np.max(np.abs(g - gw)) <= 1e-4 * np.abs(gw).max()
+    # every parameter group carries gradient
+    for a, b in ((co.W1, co.B1), (co.B1, co.W2), (co.W2, co.B2), (co.B2, co.W3), (co.W3, co.B3)):
+        assert np.abs(gw[a:b]).max() > 0
+    # deterministic: the same batch gives the same bits
+    g2, loss2 = tr.grad(dX.data_ptr(), dt.data_ptr(), dw.data_ptr(), n, wscale)
+    assert np.array_equal(g, g2) and loss == loss2
+    tr.close()
+
+
+def test_adam_step_matches_oracle(gpu):
+    rng = np.random.default_rng(9)
+    n = 3000
+    X = rng.standard_normal((n, 9)).astype(np.float32)
+    t = rng.uniform(0, 3, n).astype(np.float32)
+    w = np.ones(n, np.float32)
+    net = _net(3)
+    tr = gpu.Trainer(net, gpu.adam_default(lr=1e-2, weight_decay=0.01))
+    dX, dt, dw = _dev(X), _dev(t), _dev(w)
+    g, _ = tr.grad(dX.data_ptr(), dt.data_ptr(), dw.data_ptr(), n, 1.0 / n)
+    tr.adam_step()
+    got = tr.net()
+    theta0 = net[:co.NPARAM].astype(np.float64)
+    _, _, _, want = co.adam(theta0, np.zeros(co.NPARAM), np.zeros(co.NPARAM), g.astype(np.float64), 1,
+                            lr=1e-2, wd=0.01)
+    k = np.arange(co.NPARAM)
+    wt = co.is_weight(k)
+    # weights: equal up to one bf16 step where fp32 and fp64 round differently
+    ulp = np.abs(want[wt]) * 2.0 ** -7 + 1e-30
+    assert np.all(np.abs(got[:co.NPARAM][wt] - want[wt]) <= ulp)
+    assert np.mean(got[:co.NPARAM][wt] == want[wt]) > 0.99
+    assert np.allclose(got[:co.NPARAM][~wt], want[~wt], rtol=1e-6, atol=1e-7)
+    assert np.array_equal(got[co.MEAN:], net[co.MEAN:])
+    tr.close()
+
+
+def test_fit_learns_a_teacher_network(gpu):
+    """Minibatch Adam over a dataset labelled by another network: the loss
+    falls by over 20x, and a second fit with the same seed is bit-identical."""
+    import torch
+    rng = np.random.default_rng(12)
+    n = 1 << 16
+    X = rng.standard_normal((n, 9)).astype(np.float32)
+    teacher = co.random_net(40)
+    dX = _dev(X)
+    t = torch.empty(n, device="cuda")
+    gpu.closure_predict(teacher, dX.data_ptr(), n, t.data_ptr())
+    w = torch.ones(n, device="cuda")
+    nets = []
+    for _ in range(2):
+        tr = gpu.Trainer(co.random_net(41), gpu.adam_default(lr=3e-3))
+        losses = tr.fit(dX.data_ptr(), t.data_ptr(), w.data_ptr(), n, 1024, 25, seed=5)
+        nets.append(tr.net())
+        tr.close()
+    assert losses[-1] < losses[0] / 20, losses
+    assert np.array_equal(nets[0], nets[1])
+
+
+def _closure_pair(lbm, oracle, shape, net, precision=0, collision=0, tau=0.52, cs=0.15, seed=1):
+    n = int(np.prod(shape))
+    d = lbm.default_desc(nx=shape[0], ny=shape[1], nz=shape[2], mode=lbm.MODE_PHYSICS,
+                         precision=precision, collision=collision, periodic=(1, 1, 1), tau=tau,
+                         smagorinsky_cs=cs)
+    lat = lbm.Lattice(d)
+    if net is not None:
+        lat.set_closure(net)
+    u = _smooth_field(shape, seed).astype(np.float32)
+    rho = np.ones(n, np.float32)
+    lat.init_from_moments(rho, np.ascontiguousarray(u.T))
+    st = oracle.ExtState(shape, periodic=(1, 1, 1), tau=tau, collision=collision, smag_cs=cs, net=net)
+    st.init(rho.astype(np.float64), u.astype(np.float64))
+    return lat, st
+
+
+@pytest.mark.parametrize("shape,coll", [((24, 10, 8), 0), ((23, 10, 8), 0), ((24, 10, 8), 1)])
+def test_closure_step_matches_ext_oracle(gpu, oracle, shape, coll):
+    """The fused step with the network in the collide (pair kernel for even
+    nx, one-node kernel for odd nx; BGK and TRT) against FP64 ExtStep with
+    the same network, 60 steps (graph launches included)."""
+    net = _net(7)
+    lat, st = _closure_pair(gpu, oracle, shape, net, collision=coll)
+    lat.step(60)
+    st.step(60)
+    rho, u = lat.read_moments()
+    scale = np.abs(st.u).max()
+    assert np.max(np.abs(u.T - st.u)) / scale <= 3e-5
+    assert np.max(np.abs(rho - st.rho)) <= 1e-5
+    # the network changed the flow: compared with plain Smagorinsky
+    ref, st2 = _closure_pair(gpu, oracle, shape, None, collision=coll)
+    ref.step(60)
+    _, u2 = ref.read_moments()
+    assert np.max(np.abs(u2 - u)) / scale > 1e-4
+    lat.close()
+    ref.close()
+
+
+def test_closure_step_f16_storage(gpu, oracle):
+    net = _net(8)
+    lat, st = _closure_pair(gpu, oracle, (32, 12, 10), net, precision=gpu.PREC_F16S)
+    lat.step(40)
+    st.step(40)
+    _, u = lat.read_moments()
+    err = np.sqrt(((u.T - st.u) ** 2).sum() / (st.u ** 2).sum())
+    assert err <= 1e-3, err
+
+
+def test_unit_network_is_smagorinsky(gpu):
+    """r = 1 everywhere (up to the float32 b3) reproduces plain Smagorinsky."""
+    shape = (24, 10, 8)
+    outs = []
+    for net in (co.unit_net(), None):
+        n = int(np.prod(shape))
+        d = gpu.default_desc(nx=24, ny=10, nz=8, mode=gpu.MODE_PHYSICS, periodic=(1, 1, 1), tau=0.52,
+                             smagorinsky_cs=0.15)
+        lat = gpu.Lattice(d)
+        if net is not None:
+            lat.set_closure(net)
+        u = _smooth_field(shape, 1).astype(np.float32)
+        lat.init_from_moments(np.ones(n, np.float32), np.ascontiguousarray(u.T))
+        lat.step(50)
+        outs.append(lat.read_moments()[1])
+        lat.close()
+    assert np.max(np.abs(outs[0] - outs[1])) <= 1e-6 * np.abs(outs[1]).max()
+
+
+def test_set_closure_rules_and_graph_refresh(gpu):
+    net = _net(9)
+    # no Smagorinsky constant to scale
+    lat = gpu.Lattice(mode=gpu.MODE_PHYSICS, periodic=(1, 1, 1), tau=0.55)
+    with pytest.raises(gpu.LbmError) as e:
+        lat.set_closure(net)
+    assert e.value.code == gpu.ERR_INVALID_ARG
+    lat.close()
+    lat = gpu.Lattice(mode=gpu.MODE_PHYSICS, periodic=(1, 1, 1), tau=0.55, smagorinsky_cs=0.1,
+                      body_accel=(1e-6, 0, 0))
+    with pytest.raises(gpu.LbmError) as e:
+        lat.set_closure(net)
+    assert e.value.code == gpu.ERR_UNSUPPORTED
+    lat.close()
+    lat = gpu.Lattice()  # reference mode
+    with pytest.raises(gpu.LbmError) as e:
+        lat.set_closure(net)
+    assert e.value.code == gpu.ERR_UNSUPPORTED
+    lat.close()
+    bad = net.copy()
+    bad[5] = np.nan
+    lat = gpu.Lattice(mode=gpu.MODE_PHYSICS, periodic=(1, 1, 1), tau=0.55, smagorinsky_cs=0.1)
+    with pytest.raises(gpu.LbmError):
+        lat.set_closure(bad)
+    lat.close()
+    # switching networks between graph-launched steps equals single launches
+    shape = (24, 10, 8)
+    n = int(np.prod(shape))
+    u = np.ascontiguousarray(_smooth_field(shape, 2).astype(np.float32).T)
+    pops = []
+    for single in (False, True):
+        lat = gpu.Lattice(nx=24, ny=10, nz=8, mode=gpu.MODE_PHYSICS, periodic=(1, 1, 1), tau=0.52,
+                          smagorinsky_cs=0.15)
+        lat.init_from_moments(np.ones(n, np.float32), u)
+        for nn in (net, _net(10), None):
+            lat.set_closure(nn)
+            if single:
+                for _ in range(40):
+                    lat.step(1)
+            else:
+                lat.step(40)
+        pops.append(lat.read_populations())
+        lat.close()
+    assert np.array_equal(pops[0], pops[1])
