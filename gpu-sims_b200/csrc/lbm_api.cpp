@@ -515,6 +515,28 @@ int lbm_write_populations(lbm_ctx* c, const float* f, size_t n) {
   return LBM_OK;
 }
 
+int lbm_read_mask(lbm_ctx* c, uint8_t* mask, size_t n) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!mask || n != c->n) return fail(c, LBM_ERR_INVALID_ARG, "mask must hold Nx*Ny*Nz bytes");
+  CK(cudaMemcpyAsync(mask, c->mask, n, cudaMemcpyDeviceToHost, c->stream), "read mask");
+  CK(cudaStreamSynchronize(c->stream), "read_mask sync");
+  return LBM_OK;
+}
+
+int lbm_get_desc(lbm_ctx* c, lbm_desc* desc) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!desc || desc->struct_size != sizeof(lbm_desc))
+    return fail(c, LBM_ERR_INVALID_ARG, "desc is NULL or desc.struct_size is wrong");
+  *desc = c->d;
+  return LBM_OK;
+}
+
+int lbm_set_iteration(lbm_ctx* c, uint64_t iteration) {
+  if (int rc = check_ctx(c)) return rc;
+  c->iteration = iteration;
+  return LBM_OK;
+}
+
 int lbm_get_info(lbm_ctx* c, lbm_info* info) {
   if (int rc = check_ctx(c)) return rc;
   if (!info || info->struct_size != sizeof(lbm_info))

@@ -89,6 +89,18 @@ class BatchInfo(C.Structure):
     ]
 
 
+class CaptureInfo(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_uint32), ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+        ("frame", C.c_uint32), ("iteration", C.c_uint64), ("has_populations", C.c_int32),
+        ("mask_frame_invariant", C.c_int32),
+    ]
+
+
+CAPTURE_LOAD_MASK = 1
+CAPTURE_MOMENTS_ONLY = 2
+
+
 class Adam(C.Structure):
     _fields_ = [
         ("struct_size", C.c_uint32), ("lr", C.c_float), ("beta1", C.c_float),
@@ -146,6 +158,15 @@ _SIGS = {
     "lbm_batch_autotune": (C.c_int, [_P, C.c_int, C.POINTER(BatchSchedule)]),
     "lbm_batch_get_info": (C.c_int, [_P, C.POINTER(BatchInfo)]),
     "lbm_batch_last_error": (C.c_char_p, [_P]),
+    "lbm_read_mask": (C.c_int, [_P, _P, C.c_size_t]),
+    "lbm_get_desc": (C.c_int, [_P, C.POINTER(Desc)]),
+    "lbm_set_iteration": (C.c_int, [_P, _U64]),
+    "lbm_capture_write": (C.c_int, [C.c_char_p, C.c_uint32, C.c_char_p, _I32, _I32, _I32, _P, _P, _P, _P]),
+    "lbm_capture_read": (C.c_int, [C.c_char_p, C.POINTER(CaptureInfo), _P, _P, _P, _P]),
+    "lbm_capture_latest": (C.c_int, [C.c_char_p, C.c_char_p, C.c_size_t]),
+    "lbm_capture_save": (C.c_int, [_P, C.c_char_p, C.c_uint32, C.c_char_p, C.c_int]),
+    "lbm_capture_load": (C.c_int, [_P, C.c_char_p, C.c_int]),
+    "lbm_capture_last_error": (C.c_char_p, []),
     "lbm_set_closure": (C.c_int, [_P, _P]),
     "lbm_box_filter": (C.c_int, [_P, _P, _I32, _I32, _I32, _I32, _P, _P]),
     "lbm_closure_samples": (C.c_int, [_P, _I32, _I32, _I32, _F, _F, _U64, _I64, _P, _P, _P, _P]),
@@ -276,6 +297,25 @@ class Lattice:
     def set_flags(self, mask: np.ndarray) -> None:
         m = np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
         self._c(load().lbm_set_flags(self._h, _ptr(m), m.size))
+
+    def read_mask(self) -> np.ndarray:
+        out = np.zeros(self.n, np.uint8)
+        self._c(load().lbm_read_mask(self._h, _ptr(out), out.size))
+        return out
+
+    def set_iteration(self, iteration: int) -> None:
+        self._c(load().lbm_set_iteration(self._h, iteration))
+
+    def capture_save(self, root: str, frame: int, meta: dict | None = None,
+                     full_state: bool = False) -> None:
+        """F5: writes <root>/capture_<frame>/ (see lbm_capture_save)."""
+        import json
+        m = None if meta is None else json.dumps(meta).encode()
+        self._c(load().lbm_capture_save(self._h, str(root).encode(), frame, m, int(full_state)))
+
+    def capture_load(self, capture_dir: str, flags: int = 0) -> None:
+        """F9: restores a capture (see lbm_capture_load)."""
+        self._c(load().lbm_capture_load(self._h, str(capture_dir).encode(), flags))
 
     def set_closure(self, net: np.ndarray | None) -> None:
         """Installs a learned-closure network (float[CLOSURE_FLOATS]); None
@@ -580,3 +620,57 @@ class Trainer:
         out = np.empty(CLOSURE_FLOATS, np.float32)
         self._c(load().lbm_trainer_get_net(self._h, _ptr(out)))
         return out
+
+
+# ---- capture directories (include/lbm.h) -------------------------------------
+
+def _cap_check(rc: int) -> None:
+    if rc != OK:
+        raise LbmError(rc, load().lbm_capture_last_error().decode())
+
+
+def capture_write(root: str, frame: int, shape, rho: np.ndarray, vel_rgba16f: np.ndarray,
+                  mask: np.ndarray, pops: np.ndarray | None = None, meta: dict | None = None) -> None:
+    """Writes a capture from host arrays (no device needed)."""
+    import json
+    nx, ny, nz = shape
+    n = nx * ny * nz
+    r = np.ascontiguousarray(rho, np.float32).reshape(-1)
+    v = np.ascontiguousarray(vel_rgba16f).view(np.uint16).reshape(-1)
+    m = np.ascontiguousarray(mask, np.uint8).reshape(-1)
+    if r.size != n or v.size != 4 * n or m.size != n:
+        raise LbmError(ERR_INVALID_ARG, "capture_write: array sizes do not match the shape")
+    p = None
+    if pops is not None:
+        p = np.ascontiguousarray(pops, np.float32).reshape(-1)
+        if p.size != 19 * n:
+            raise LbmError(ERR_INVALID_ARG, "capture_write: populations must be float[19][N]")
+    mj = None if meta is None else json.dumps(meta).encode()
+    _cap_check(load().lbm_capture_write(str(root).encode(), frame, mj, nx, ny, nz, _ptr(r), _ptr(v),
+                                        _ptr(m), None if p is None else _ptr(p)))
+
+
+def capture_read(capture_dir: str) -> dict:
+    """Parses a capture: dict with the info fields and the arrays density
+    float32[N], velocity uint16[N][4] (rgba16f bits), obstacle_mask
+    uint8[N] and populations float32[19][N] (None if absent)."""
+    info = CaptureInfo()
+    info.struct_size = C.sizeof(CaptureInfo)
+    d = str(capture_dir).encode()
+    _cap_check(load().lbm_capture_read(d, C.byref(info), None, None, None, None))
+    n = info.nx * info.ny * info.nz
+    rho = np.empty(n, np.float32)
+    vel = np.empty((n, 4), np.uint16)
+    mask = np.empty(n, np.uint8)
+    pops = np.empty((19, n), np.float32) if info.has_populations else None
+    _cap_check(load().lbm_capture_read(d, C.byref(info), _ptr(rho), _ptr(vel), _ptr(mask),
+                                       None if pops is None else _ptr(pops)))
+    return {"shape": (info.nx, info.ny, info.nz), "frame": info.frame, "iteration": info.iteration,
+            "mask_frame_invariant": bool(info.mask_frame_invariant), "density": rho, "velocity": vel,
+            "obstacle_mask": mask, "populations": pops}
+
+
+def capture_latest(root: str) -> str:
+    buf = C.create_string_buffer(4096)
+    _cap_check(load().lbm_capture_latest(str(root).encode(), buf, 4096))
+    return buf.value.decode()

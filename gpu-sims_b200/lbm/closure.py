@@ -115,24 +115,161 @@ def _events():
     return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
 
-def _coarse_run(lbm, stream, nc, tau_c, cs0, rho0, u0, steps, eval_every, net=None):
-    """Coarse periodic BGK-Smagorinsky run (learned closure when net is
-    given) from host moments; returns (device seconds of the steps, spectra
-    at every eval_every steps, kinetic energy there)."""
+class FineRun:
+    """A fine periodic plain-BGK HIT run and what the closure needs from it:
+    the filtered initial field, filtered spectra and kinetic energy every
+    `eval_every` coarse steps, and (collect=True) the training samples on the
+    device."""
+
+    def __init__(self, fine=512, factor=4, tau_f=0.508, snapshots=2000, every=8,
+                 samples_per_snapshot=4096, cs0=0.1, seed=5, u_rms=0.04, eval_every=250,
+                 collect=True, stream=None):
+        import torch
+
+        import lbm
+        self.fine, self.factor, self.tau_f, self.seed = fine, factor, tau_f, seed
+        self.nc = nc = fine // factor
+        self.tau_c = 0.5 + (tau_f - 0.5) / factor
+        self.steps_c = snapshots * every // factor
+        self.eval_every = eval_every
+        stream = stream or torch.cuda.current_stream()
+        sptr = stream.cuda_stream
+        u = hit_velocity(fine, seed, u_rms)
+        uh = u.permute(1, 2, 3, 0).reshape(-1, 3).contiguous().cpu().numpy()
+        del u
+        torch.cuda.empty_cache()
+        d = lbm.default_desc(nx=fine, ny=fine, nz=fine, mode=lbm.MODE_PHYSICS,
+                             precision=lbm.PREC_F32, collision=lbm.COLL_BGK, tau=tau_f,
+                             periodic=(1, 1, 1))
+        lat = lbm.Lattice(d)
+        lat.set_stream(sptr)
+        lat.init_from_moments(np.ones(fine ** 3, np.float32), uh)
+        del uh
+        d_rho, d_u = lat.device_moments()
+        filt = torch.empty((10, nc ** 3), device="cuda")
+        lbm.box_filter(d_rho, d_u, (fine,) * 3, factor, filt.data_ptr(), sptr)
+        torch.cuda.synchronize()
+        self.filt0 = filt.cpu().numpy()
+        self.spectra = {0: spectrum(filt[1:4].reshape(3, nc, nc, nc))}
+        self.ke = {0: float(0.5 * (filt[1:4].double() ** 2).sum(0).mean())}
+        m = samples_per_snapshot
+        self.n_samples = snapshots * m if collect else 0
+        if collect:
+            self.X = torch.empty((snapshots * m, lbm.CLOSURE_INPUTS), device="cuda")
+            self.T = torch.empty(snapshots * m, device="cuda")
+            self.W = torch.empty(snapshots * m, device="cuda")
+        self.step_s = 0.0
+        t_wall = _events()
+        t_wall[0].record(stream)
+        for s in range(snapshots):
+            e0, e1 = _events()
+            e0.record(stream)
+            lat.step(every)
+            e1.record(stream)
+            step_c = (s + 1) * every // factor
+            want_spec = ((s + 1) * every) % factor == 0 and step_c % eval_every == 0
+            if collect or want_spec:
+                lbm.box_filter(d_rho, d_u, (fine,) * 3, factor, filt.data_ptr(), sptr)
+            if collect:
+                lbm.closure_samples(filt.data_ptr(), (nc,) * 3, self.tau_c, cs0,
+                                    1000003 * (s + 1) + seed, m, self.X[s * m].data_ptr(),
+                                    self.T[s * m:].data_ptr(), self.W[s * m:].data_ptr(), sptr)
+            if want_spec:
+                self.spectra[step_c] = spectrum(filt[1:4].reshape(3, nc, nc, nc))
+                self.ke[step_c] = float(0.5 * (filt[1:4].double() ** 2).sum(0).mean())
+            e1.synchronize()
+            self.step_s += e0.elapsed_time(e1) / 1e3
+        t_wall[1].record(stream)
+        lat.sync()
+        torch.cuda.synchronize()
+        self.total_s = t_wall[0].elapsed_time(t_wall[1]) / 1e3
+        lat.close()
+
+    def free(self):
+        for k in ("X", "T", "W"):
+            if hasattr(self, k):
+                delattr(self, k)
+
+
+def train(fr: FineRun, epochs=20, batch=4096, lr=1e-3, seed=5, target_clip=50.0, stream=None):
+    """Fits a network to the run's samples; returns (network, info)."""
     import torch
+
+    import lbm
+    stream = stream or torch.cuda.current_stream()
+    X, T, W = fr.X, fr.T, fr.W
+    T.clamp_(-target_clip, target_clip)
+    w64 = W.double()
+    r_data = float((w64 * T.double()).sum() / w64.sum())
+    mean = X.double().mean(0).float().cpu().numpy()
+    std = X.double().std(0).float().cpu().numpy()
+    iscale = (1.0 / np.maximum(std, 1e-6)).astype(np.float32)
+    tr = lbm.Trainer(init_net(seed, mean, iscale), lbm.adam_default(lr=lr))
+    tr.set_stream(stream.cuda_stream)
+    e0, e1 = _events()
+    e0.record(stream)
+    losses = tr.fit(X.data_ptr(), T.data_ptr(), W.data_ptr(), fr.n_samples, batch, epochs, seed=seed)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    train_s = e0.elapsed_time(e1) / 1e3
+    net = tr.net()
+    tr.close()
+    R = torch.empty(fr.n_samples, device="cuda")
+    lbm.closure_predict(net, X.data_ptr(), fr.n_samples, R.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    r_net = float((w64 * R.double()).sum() / w64.sum())
+    return net, {"epochs": epochs, "batch": batch, "lr": lr, "train_s": train_s,
+                 "loss": [float(x) for x in losses], "r_weighted_data": r_data,
+                 "r_weighted_net": r_net, "samples": fr.n_samples}
+
+
+def constant_net(r: float, like: np.ndarray) -> np.ndarray:
+    """A network whose output is the constant r (zero weights, b3 =
+    softplus^-1(r)); the standardisation is copied from `like`."""
+    import lbm
+    w = np.zeros(lbm.CLOSURE_FLOATS, np.float32)
+    w[lbm.CLOSURE_PARAMS - 1] = math.log(math.expm1(r))
+    w[lbm.CLOSURE_PARAMS:] = like[lbm.CLOSURE_PARAMS:]
+    return w
+
+
+def apriori_loss(net: np.ndarray, fr: FineRun, stream=None) -> float:
+    """Weighted mean squared error sum w (r(x) - r*)^2 / sum w of a network
+    over a run's samples (the fused forward/backward kernel's loss)."""
+    import torch
+
+    import lbm
+    stream = stream or torch.cuda.current_stream()
+    wsum = float(fr.W.double().sum())
+    tr = lbm.Trainer(net)
+    tr.set_stream(stream.cuda_stream)
+    _, loss = tr.grad(fr.X.data_ptr(), fr.T.data_ptr(), fr.W.data_ptr(), fr.n_samples, 1.0 / wsum)
+    tr.close()
+    return loss
+
+
+def coarse_run(fr: FineRun, cs: float, net=None, stream=None):
+    """Coarse periodic BGK-Smagorinsky run (constant `cs`, or the learned
+    closure with Cs^2 = cs^2 r when `net` is given) from the run's filtered
+    initial field; device seconds of the steps, spectra and kinetic energy
+    every eval_every steps."""
+    import torch
+
+    import lbm
+    stream = stream or torch.cuda.current_stream()
+    nc = fr.nc
     d = lbm.default_desc(nx=nc, ny=nc, nz=nc, mode=lbm.MODE_PHYSICS, precision=lbm.PREC_F32,
-                         collision=lbm.COLL_BGK, tau=tau_c, periodic=(1, 1, 1), smagorinsky_cs=cs0)
+                         collision=lbm.COLL_BGK, tau=fr.tau_c, periodic=(1, 1, 1), smagorinsky_cs=cs)
     lat = lbm.Lattice(d)
     lat.set_stream(stream.cuda_stream)
     if net is not None:
         lat.set_closure(net)
-    lat.init_from_moments(rho0, u0)
-    secs, spectra, ke = 0.0, {}, {}
-    ok = True
-    for s in range(0, steps, eval_every):
+    lat.init_from_moments(np.ascontiguousarray(fr.filt0[0]), np.ascontiguousarray(fr.filt0[1:4].T))
+    secs, spectra, ke, ok = 0.0, {}, {}, True
+    for s in range(0, fr.steps_c, fr.eval_every):
         e0, e1 = _events()
         e0.record(stream)
-        lat.step(eval_every)
+        lat.step(fr.eval_every)
         e1.record(stream)
         try:
             lat.sync()
@@ -142,139 +279,98 @@ def _coarse_run(lbm, stream, nc, tau_c, cs0, rho0, u0, steps, eval_every, net=No
         torch.cuda.synchronize()
         secs += e0.elapsed_time(e1) / 1e3
         _, u = lat.read_moments()
-        spectra[s + eval_every] = spectrum_np(u, nc)
-        ke[s + eval_every] = float(0.5 * np.mean(np.sum(u.astype(np.float64) ** 2, axis=1)))
+        spectra[s + fr.eval_every] = spectrum_np(u, nc)
+        ke[s + fr.eval_every] = float(0.5 * np.mean(np.sum(u.astype(np.float64) ** 2, axis=1)))
     lat.close()
     return {"device_s": secs, "spectra": spectra, "ke": ke, "finite": ok}
+
+
+def errors(run: dict, fr: FineRun, kmax: int = 16) -> dict:
+    """Relative spectral errors |E_c(k) - E_f(k)| / E_f(k), 1 <= k <= kmax,
+    against the filtered fine run at matching times: at the last time
+    (max and mean over k) and averaged over all times."""
+    k = np.arange(1, kmax + 1)
+    errs = {t: np.abs(e[k] - fr.spectra[t][k]) / fr.spectra[t][k]
+            for t, e in run["spectra"].items() if t in fr.spectra}
+    if not run["finite"] or not errs:
+        return {"finite": False}
+    last = max(errs)
+    return {"finite": True, "device_s": run["device_s"],
+            "final_max": float(errs[last].max()), "final_mean": float(errs[last].mean()),
+            "time_mean": float(np.mean([v.mean() for v in errs.values()])),
+            "time_max": float(max(v.max() for v in errs.values())),
+            "ke_ratio": {str(t): run["ke"][t] / fr.ke[t] for t in run["ke"] if t in fr.ke},
+            "by_time": {str(t): [float(x) for x in v] for t, v in errs.items()}}
 
 
 def run(fine: int = 512, factor: int = 4, tau_f: float = 0.508, snapshots: int = 2000,
         every: int = 8, samples_per_snapshot: int = 4096, cs0: float = 0.1, seed: int = 5,
         u_rms: float = 0.04, epochs: int = 20, batch: int = 4096, lr: float = 1e-3,
-        eval_every: int = 250, kmax: int = 16, target_clip: float = 50.0, verbose: bool = True) -> dict:
-    """The whole experiment (module docstring); returns the results dict."""
+        eval_every: int = 250, kmax: int = 16,
+        calibrate=(0.25, 0.5, 0.75, 1.0, 1.5, 2.0, 3.0, 4.0, 6.0), verbose: bool = True) -> dict:
+    """The experiment: a training run (seed) gives the samples and, by a
+    sweep of a single scale on Cs0 against its own filtered spectra, the
+    calibration of the learned closure; a held-out run (seed + 1) is the
+    evaluation: Smagorinsky Cs0 and the learned closure from its filtered
+    initial field, compared with its filtered spectra."""
     import torch
-
-    import lbm
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    sptr = stream.cuda_stream
-    nc = fine // factor
-    tau_c = 0.5 + (tau_f - 0.5) / factor
-    steps_c = snapshots * every // factor
     log = (lambda *a: print(*a, flush=True)) if verbose else (lambda *a: None)
-
-    # 1. initial field and the fine lattice
-    u = hit_velocity(fine, seed, u_rms)
-    uh = u.permute(1, 2, 3, 0).reshape(-1, 3).contiguous().cpu().numpy()
-    del u
-    torch.cuda.empty_cache()
-    d = lbm.default_desc(nx=fine, ny=fine, nz=fine, mode=lbm.MODE_PHYSICS, precision=lbm.PREC_F32,
-                         collision=lbm.COLL_BGK, tau=tau_f, periodic=(1, 1, 1))
-    lat = lbm.Lattice(d)
-    lat.set_stream(sptr)
-    lat.init_from_moments(np.ones(fine ** 3, np.float32), uh)
-    del uh
-    d_rho, d_u = lat.device_moments()
-    filt = torch.empty((10, nc ** 3), device="cuda")
-    lbm.box_filter(d_rho, d_u, (fine,) * 3, factor, filt.data_ptr(), sptr)
-    torch.cuda.synchronize()
-    filt0 = filt.cpu().numpy()
-    fine_spectra = {0: spectrum(filt[1:4].reshape(3, nc, nc, nc))}
-    fine_ke = {0: float(0.5 * (filt[1:4].double() ** 2).sum(0).mean())}
-
-    # 2. fine run, filtered snapshots, training samples
-    m = samples_per_snapshot
-    X = torch.empty((snapshots * m, lbm.CLOSURE_INPUTS), device="cuda")
-    T = torch.empty(snapshots * m, device="cuda")
-    W = torch.empty(snapshots * m, device="cuda")
-    step_s = 0.0
-    t_wall = _events()
-    t_wall[0].record(stream)
-    for s in range(snapshots):
-        e0, e1 = _events()
-        e0.record(stream)
-        lat.step(every)
-        e1.record(stream)
-        lbm.box_filter(d_rho, d_u, (fine,) * 3, factor, filt.data_ptr(), sptr)
-        lbm.closure_samples(filt.data_ptr(), (nc,) * 3, tau_c, cs0, 1000003 * (s + 1) + seed, m,
-                            X[s * m].data_ptr(), T[s * m:].data_ptr(), W[s * m:].data_ptr(), sptr)
-        step_c = (s + 1) * every // factor
-        if ((s + 1) * every) % factor == 0 and step_c % eval_every == 0:
-            fine_spectra[step_c] = spectrum(filt[1:4].reshape(3, nc, nc, nc))
-            fine_ke[step_c] = float(0.5 * (filt[1:4].double() ** 2).sum(0).mean())
-        e1.synchronize()
-        step_s += e0.elapsed_time(e1) / 1e3
-    t_wall[1].record(stream)
-    lat.sync()
-    torch.cuda.synchronize()
-    fine_total_s = t_wall[0].elapsed_time(t_wall[1]) / 1e3
-    lat.close()
-    log(f"fine {fine}^3: {snapshots * every} steps, step time {step_s:.1f} s, with data {fine_total_s:.1f} s")
-
-    # 3. training
-    T.clamp_(-target_clip, target_clip)
-    w64 = W.double()
-    r_eff = float((w64 * T.double()).sum() / w64.sum())
-    mean = X.double().mean(0).float().cpu().numpy()
-    std = X.double().std(0).float().cpu().numpy()
-    iscale = (1.0 / np.maximum(std, 1e-6)).astype(np.float32)
-    tr = lbm.Trainer(init_net(seed, mean, iscale), lbm.adam_default(lr=lr))
-    tr.set_stream(sptr)
-    e0, e1 = _events()
-    e0.record(stream)
-    losses = tr.fit(X.data_ptr(), T.data_ptr(), W.data_ptr(), snapshots * m, batch, epochs, seed=seed)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    train_s = e0.elapsed_time(e1) / 1e3
-    net = tr.net()
-    tr.close()
-    # network output over the dataset, for the record
-    R = torch.empty(snapshots * m, device="cuda")
-    lbm.closure_predict(net, X.data_ptr(), snapshots * m, R.data_ptr(), sptr)
-    torch.cuda.synchronize()
-    r_pred_w = float((w64 * R.double()).sum() / w64.sum())
-    log(f"training: {epochs} epochs in {train_s:.2f} s, loss {losses[0]:.4g} -> {losses[-1]:.4g}; "
-        f"weighted r*: data {r_eff:.3f}, network {r_pred_w:.3f}")
-    del X, T, W, R
-
-    # 4. coarse runs from the filtered initial field
-    rho0 = np.ascontiguousarray(filt0[0])
-    u0 = np.ascontiguousarray(filt0[1:4].T)
-    runs = {"smagorinsky": _coarse_run(lbm, stream, nc, tau_c, cs0, rho0, u0, steps_c, eval_every),
-            "learned": _coarse_run(lbm, stream, nc, tau_c, cs0, rho0, u0, steps_c, eval_every, net)}
-
-    # 5. spectra errors against the filtered fine field
-    res = {"fine": fine, "factor": factor, "coarse": nc, "tau_fine": tau_f, "tau_coarse": tau_c,
-           "fine_steps": snapshots * every, "coarse_steps": steps_c, "cs0": cs0, "u_rms": u_rms,
-           "samples": snapshots * m, "epochs": epochs, "batch": batch, "lr": lr,
-           "train_s": train_s, "loss_first": float(losses[0]), "loss_last": float(losses[-1]),
-           "r_weighted_data": r_eff, "r_weighted_net": r_pred_w,
-           "fine_step_s": step_s, "fine_total_s": fine_total_s, "kmax": kmax}
-    for name, r in runs.items():
-        errs = {}
-        for t, e in r["spectra"].items():
-            ef = fine_spectra.get(t)
-            if ef is None:
-                continue
-            k = np.arange(1, kmax + 1)
-            errs[t] = np.abs(e[k] - ef[k]) / ef[k]
-        final = max(errs) if errs else None
-        res[name] = {
-            "finite": r["finite"], "device_s": r["device_s"],
-            "wall_ratio": step_s / r["device_s"] if r["device_s"] else None,
-            "max_rel_err_final": float(errs[final].max()) if final else None,
-            "mean_rel_err_final": float(errs[final].mean()) if final else None,
-            "max_rel_err_all_times": float(max(v.max() for v in errs.values())) if errs else None,
-            "mean_rel_err_all_times": float(np.mean([v.mean() for v in errs.values()])) if errs else None,
-            "ke": {str(t): v for t, v in r["ke"].items()},
-            "err_by_time": {str(t): [float(x) for x in v] for t, v in errs.items()},
-        }
-        log(f"{name}: finite {r['finite']}, {r['device_s']:.2f} s, max rel err k<={kmax} final "
-            f"{res[name]['max_rel_err_final']}, all times {res[name]['max_rel_err_all_times']}")
-    res["fine_ke"] = {str(t): v for t, v in fine_ke.items()}
-    res["fine_spectrum_final"] = [float(x) for x in fine_spectra[max(fine_spectra)][: kmax + 1]]
-    res["net"] = [float(x) for x in net]
+    common = dict(fine=fine, factor=factor, tau_f=tau_f, snapshots=snapshots, every=every,
+                  samples_per_snapshot=samples_per_snapshot, cs0=cs0, u_rms=u_rms,
+                  eval_every=eval_every, stream=stream)
+    tr_run = FineRun(seed=seed, collect=True, **common)
+    log(f"training run {fine}^3 seed {seed}: {snapshots * every} steps in {tr_run.step_s:.1f} s")
+    net, info = train(tr_run, epochs=epochs, batch=batch, lr=lr, seed=seed, stream=stream)
+    r_const = info["r_weighted_data"]
+    info["apriori_train"] = {"network": apriori_loss(net, tr_run, stream),
+                             "best_constant": apriori_loss(constant_net(r_const, net), tr_run, stream),
+                             "smagorinsky": apriori_loss(constant_net(1.0, net), tr_run, stream)}
+    tr_run.free()
+    log(f"training: {info['train_s']:.2f} s, loss {info['loss'][0]:.4g} -> {info['loss'][-1]:.4g}, "
+        f"weighted r: data {info['r_weighted_data']:.3f} network {info['r_weighted_net']:.3f}")
+    # calibration on the training run: one scale s on Cs0 (Cs^2 = s^2 cs0^2 r)
+    cal = {}
+    for a in calibrate:
+        e = errors(coarse_run(tr_run, cs0 * math.sqrt(a), net, stream), tr_run, kmax)
+        cal[a] = e
+        log(f"  calibration alpha {a}: time-mean err {e.get('time_mean')}")
+    best = min((a for a in cal if cal[a]["finite"]), key=lambda a: cal[a]["time_mean"])
+    # the same one-scale calibration of plain Smagorinsky, for comparison
+    cal_s = {}
+    for a in calibrate:
+        cal_s[a] = errors(coarse_run(tr_run, cs0 * math.sqrt(a), None, stream), tr_run, kmax)
+        log(f"  Smagorinsky alpha {a}: time-mean err {cal_s[a].get('time_mean')}")
+    best_s = min((a for a in cal_s if cal_s[a]["finite"]), key=lambda a: cal_s[a]["time_mean"])
+    ev_run = FineRun(seed=seed + 1, collect=True, **common)
+    log(f"evaluation run seed {seed + 1}: {ev_run.step_s:.1f} s")
+    ev_run.T.clamp_(-50.0, 50.0)
+    info["apriori_heldout"] = {"network": apriori_loss(net, ev_run, stream),
+                               "best_constant": apriori_loss(constant_net(r_const, net), ev_run, stream),
+                               "smagorinsky": apriori_loss(constant_net(1.0, net), ev_run, stream)}
+    log(f"a-priori weighted MSE on the held-out run: {info['apriori_heldout']}")
+    ev_run.free()
+    res = {"fine": fine, "factor": factor, "coarse": ev_run.nc, "tau_fine": tau_f,
+           "tau_coarse": ev_run.tau_c, "fine_steps": snapshots * every, "coarse_steps": ev_run.steps_c,
+           "cs0": cs0, "u_rms": u_rms, "kmax": kmax, "train_seed": seed, "eval_seed": seed + 1,
+           "training": info, "calibration": {str(a): {k: v for k, v in e.items() if k != "by_time"}
+                                              for a, e in cal.items()},
+           "calibration_smagorinsky": {str(a): {k: v for k, v in e.items() if k != "by_time"}
+                                        for a, e in cal_s.items()},
+           "alpha": best, "alpha_smagorinsky": best_s, "fine_step_s": ev_run.step_s, "fine_total_s": ev_run.total_s,
+           "fine_ke": {str(t): v for t, v in ev_run.ke.items()},
+           "fine_spectrum_final": [float(x) for x in ev_run.spectra[max(ev_run.spectra)][: kmax + 1]],
+           "net": [float(x) for x in net]}
+    for name, cs, nn in (("smagorinsky", cs0, None), ("learned", cs0 * math.sqrt(best), net),
+                         ("learned_uncalibrated", cs0, net),
+                         ("smagorinsky_calibrated", cs0 * math.sqrt(best_s), None)):
+        e = errors(coarse_run(ev_run, cs, nn, stream), ev_run, kmax)
+        if e.get("device_s"):
+            e["wall_ratio"] = ev_run.step_s / e["device_s"]
+        res[name] = e
+        log(f"{name}: final max {e.get('final_max')}, final mean {e.get('final_mean')}, "
+            f"time mean {e.get('time_mean')}, wall ratio {e.get('wall_ratio')}")
     return res
 
 
@@ -304,9 +400,10 @@ def main(argv=None) -> int:
     if a.out:
         with open(a.out, "w") as f:
             json.dump(res, f)
-    brief = {k: v for k, v in res.items() if k not in ("net",)}
-    for name in ("smagorinsky", "learned"):
-        brief[name] = {k: v for k, v in res[name].items() if k not in ("err_by_time", "ke")}
+    brief = {k: v for k, v in res.items() if k not in ("net", "calibration", "calibration_smagorinsky")}
+    for name in ("smagorinsky", "learned", "learned_uncalibrated", "smagorinsky_calibrated"):
+        brief[name] = {k: v for k, v in res[name].items() if k not in ("by_time", "ke_ratio")}
+    brief["training"] = {k: v for k, v in res["training"].items() if k != "loss"}
     print(json.dumps(brief))
     return 0
 

@@ -202,6 +202,75 @@ LBM_API const char* lbm_last_error(lbm_ctx* ctx);
 LBM_API int lbm_conservation_noalloc(const float* d_rho, const float* d_u, size_t n,
                                      double out[4], void* stream);
 
+/* The obstacle mask as last uploaded by lbm_set_flags (all zero = all fluid
+ * before any upload).  Replaces obstacle_mask.readback in capture_save
+ * (src/main.cpp:1296). */
+LBM_API int lbm_read_mask(lbm_ctx* ctx, uint8_t* mask, size_t n);
+
+/* The descriptor the context was created with. */
+LBM_API int lbm_get_desc(lbm_ctx* ctx, lbm_desc* desc);
+
+/* Sets the step counter reported by lbm_get_info (a capture resume restores
+ * the captured iteration, as capture_load does with rt.iteration,
+ * src/main.cpp:1357). */
+LBM_API int lbm_set_iteration(lbm_ctx* ctx, uint64_t iteration);
+
+/* ---- capture directories ----------------------------------------------- */
+/* The capture layout of the reference's F5 / F9 handlers
+ * (src/main.cpp:1267-1390) and its StateWriter / StateReader
+ * (common/common-cpp/src/state_writer.cpp:26-85, state_reader.cpp:12-85):
+ * <root>/capture_%04u/state.json with {"frame", "meta": {"latticeBoltzmann":
+ * {...}}, "buffers": [...]} and one raw <name>.bin per buffer:
+ *   density        r32f     float[N]
+ *   velocity       rgba16f  uint16 half[N][4], w = 0
+ *   obstacle_mask  r8uint   uint8[N], "frame_invariant": true
+ *   populations    r32f     float[19][N], shape [19, Nx, Ny, Nz],
+ *                           post-collision f (full-state
+ *                           checkpoint; not in the reference, which cannot
+ *                           resume exactly, docs/tier1-capture-format-
+ *                           reference.md:124-134)
+ * N = Nx*Ny*Nz, x fastest.  state.json is written as nlohmann's dump(2)
+ * writes it (sorted keys, two-space indent). */
+typedef struct lbm_capture_info {
+    uint32_t struct_size;
+    int32_t  nx, ny, nz;
+    uint32_t frame;
+    uint64_t iteration;            /* latticeBoltzmann.iteration, 0 if absent */
+    int32_t  has_populations;
+    int32_t  mask_frame_invariant;
+} lbm_capture_info;
+
+#define LBM_CAPTURE_LOAD_MASK    1  /* upload the captured obstacle mask      */
+#define LBM_CAPTURE_MOMENTS_ONLY 2  /* ignore populations: f = feq(rho, u),
+                                       the reference's F9 intent              */
+
+/* Writes <root>/capture_<frame>/ from host arrays (no device needed).
+ * meta_json: the latticeBoltzmann object as JSON text (NULL: a minimal one
+ * with schemaVersion, Nx, Ny, Nz, iteration, substeps); pops may be NULL. */
+LBM_API int lbm_capture_write(const char* root, uint32_t frame, const char* meta_json,
+                              int32_t nx, int32_t ny, int32_t nz, const float* rho,
+                              const uint16_t* vel, const uint8_t* mask, const float* pops);
+/* Parses a capture directory; fills info and copies whichever buffers have a
+ * non-NULL destination (sizes from info's dimensions).  LBM_ERR_IO for a
+ * missing or malformed state.json, a missing required buffer or a file whose
+ * size is not what its dimensions give. */
+LBM_API int lbm_capture_read(const char* dir, lbm_capture_info* info, float* rho,
+                             uint16_t* vel, uint8_t* mask, float* pops);
+/* Lexicographically last capture_* directory under root (StateReader::
+ * findLatest, state_reader.cpp:12-28), as a path in out[cap]. */
+LBM_API int lbm_capture_latest(const char* root, char* out, size_t cap);
+/* F5: reads the lattice's moments (rgba16f velocity), mask and, with
+ * full_state, its populations, and writes a capture (meta_json as above;
+ * NULL: the minimal meta with the context's iteration and tau). */
+LBM_API int lbm_capture_save(lbm_ctx* ctx, const char* root, uint32_t frame,
+                             const char* meta_json, int full_state);
+/* F9: restores a capture into a lattice of the same dimensions: the mask
+ * (with LBM_CAPTURE_LOAD_MASK), then the populations if the capture has them
+ * (an exact resume) or else f = feq(rho, u) from the stored moments; the
+ * iteration counter from the meta. */
+LBM_API int lbm_capture_load(lbm_ctx* ctx, const char* dir, int flags);
+LBM_API const char* lbm_capture_last_error(void);
+
 /* ---- batched ensemble --------------------------------------------------- */
 /* Hundreds of independent physics-mode domains of uneven size advanced
  * together: one launch per step over a tile work-list (captured in a CUDA
