@@ -406,6 +406,10 @@ JVal default_meta(int nx, int ny, int nz, uint64_t iteration, double tau) {
   return m;
 }
 
+int write_capture(const char* root, uint32_t frame, const char* meta_json, int32_t nx, int32_t ny,
+                  int32_t nz, const float* rho, const uint16_t* vel, const uint8_t* mask, const float* pops,
+                  bool shifted);
+
 }  // namespace
 
 extern "C" {
@@ -413,6 +417,16 @@ extern "C" {
 int lbm_capture_write(const char* root, uint32_t frame, const char* meta_json, int32_t nx, int32_t ny,
                       int32_t nz, const float* rho, const uint16_t* vel, const uint8_t* mask,
                       const float* pops) {
+  return write_capture(root, frame, meta_json, nx, ny, nz, rho, vel, mask, pops, false);
+}
+
+}  // extern "C"
+
+namespace {
+
+int write_capture(const char* root, uint32_t frame, const char* meta_json, int32_t nx, int32_t ny,
+                  int32_t nz, const float* rho, const uint16_t* vel, const uint8_t* mask, const float* pops,
+                  bool shifted) {
   if (!root || !rho || !vel || !mask) return cfail(LBM_ERR_INVALID_ARG, "capture write: NULL argument");
   if (nx < 1 || ny < 1 || nz < 1) return cfail(LBM_ERR_INVALID_ARG, "capture write: bad dimensions");
   const size_t N = (size_t)nx * ny * nz;
@@ -461,6 +475,7 @@ int lbm_capture_write(const char* root, uint32_t frame, const char* meta_json, i
       d.o["shape"].a.insert(d.o["shape"].a.begin(), jnum(19));
       d.o["components"] = jnum(19);
       d.o["layout"] = jstr("direction-major f[19][Nx*Ny*Nz], x fastest, post-collision");
+      if (shifted) d.o["values"] = jstr("f - w");
     }
     bufs.a.push_back(std::move(d));
   }
@@ -471,6 +486,10 @@ int lbm_capture_write(const char* root, uint32_t frame, const char* meta_json, i
     return cfail(LBM_ERR_IO, "capture write: cannot write state.json");
   return LBM_OK;
 }
+
+}  // namespace
+
+extern "C" {
 
 int lbm_capture_read(const char* dir, lbm_capture_info* info, float* rho, uint16_t* vel, uint8_t* mask,
                      float* pops) {
@@ -533,9 +552,12 @@ int lbm_capture_save(lbm_ctx* ctx, const char* root, uint32_t frame, const char*
   std::vector<float> pops;
   if (int rc = lbm_read_moments(ctx, rho.data(), vel.data(), LBM_U_F16X4)) return rc;
   if (int rc = lbm_read_mask(ctx, mask.data(), N)) return rc;
+  const bool shifted = full_state && inf.mode == LBM_MODE_PHYSICS;
   if (full_state) {
     pops.resize(19 * N);
-    if (int rc = lbm_read_populations(ctx, pops.data(), 19 * N)) return rc;
+    const int rc = shifted ? lbm_read_populations_shifted(ctx, pops.data(), 19 * N)
+                           : lbm_read_populations(ctx, pops.data(), 19 * N);
+    if (rc) return rc;
   }
   std::string meta;
   if (!meta_json) {
@@ -546,8 +568,8 @@ int lbm_capture_save(lbm_ctx* ctx, const char* root, uint32_t frame, const char*
     dump(text, default_meta(inf.nx, inf.ny, inf.nz, inf.iteration, d.tau), 0);
     meta = text;
   }
-  return lbm_capture_write(root, frame, meta_json ? meta_json : meta.c_str(), inf.nx, inf.ny, inf.nz,
-                           rho.data(), vel.data(), mask.data(), full_state ? pops.data() : nullptr);
+  return write_capture(root, frame, meta_json ? meta_json : meta.c_str(), inf.nx, inf.ny, inf.nz, rho.data(),
+                       vel.data(), mask.data(), full_state ? pops.data() : nullptr, shifted);
 }
 
 int lbm_capture_load(lbm_ctx* ctx, const char* dir, int flags) {
@@ -573,8 +595,25 @@ int lbm_capture_load(lbm_ctx* ctx, const char* dir, int flags) {
   if (!mask.empty())
     if (int rc = lbm_set_flags(ctx, mask.data(), N)) return rc;
   if (int rc = lbm_init_from_moments(ctx, rho.data(), vel.data(), LBM_U_F16X4)) return rc;
-  if (pops)
-    if (int rc = lbm_write_populations(ctx, f.data(), 19 * N)) return rc;
+  if (pops) {
+    // f - w as stored by a physics-mode lattice, or plain f
+    Capture c;
+    if (int rc = open_capture(dir, c)) return rc;
+    const JVal* vals = c.buffer("populations")->get("values");
+    const bool shifted = vals && vals->k == JVal::Str && vals->s == "f - w";
+    int rc;
+    if (shifted && inf.mode == LBM_MODE_PHYSICS) {
+      rc = lbm_write_populations_shifted(ctx, f.data(), 19 * N);
+    } else {
+      if (shifted)  // f - w into a reference-mode lattice: add w back on the host
+        for (size_t i = 0; i < 19; ++i) {
+          const float wi = i == 0 ? 1.0f / 3.0f : (i <= 6 ? 1.0f / 18.0f : 1.0f / 36.0f);
+          for (size_t k = 0; k < N; ++k) f[i * N + k] += wi;
+        }
+      rc = lbm_write_populations(ctx, f.data(), 19 * N);
+    }
+    if (rc) return rc;
+  }
   return lbm_set_iteration(ctx, ci.iteration);
 }
 

@@ -189,3 +189,49 @@ const char* lbm_build_info(void) {
 }
 
 }  // extern "C"
+
+// Colour LUT of the velocity-magnitude pass, rgba8 [4][256][4], rows equal:
+// the cool-to-warm ramp of src/main.cpp:529-563 (dark blue, cyan, green,
+// yellow, red over four quarter ranges of t = i / 255), channels truncated
+// to bytes.
+extern "C" int lbm_colormap_lut(uint8_t* out) {
+  if (!out) return LBM_ERR_INVALID_ARG;
+  auto clamp01 = [](float v) { return v < 0.0f ? 0.0f : (v > 1.0f ? 1.0f : v); };
+  for (int i = 0; i < 256; ++i) {
+    const float t = (float)i / 255.0f;
+    float r, g, b;
+    if (t < 0.25f) {
+      const float f = t / 0.25f;
+      r = 0.05f; g = 0.05f + 0.6f * f; b = 0.4f + 0.6f * f;
+    } else if (t < 0.5f) {
+      const float f = (t - 0.25f) / 0.25f;
+      r = 0.05f; g = 0.65f + 0.3f * f; b = 1.0f - 0.7f * f;
+    } else if (t < 0.75f) {
+      const float f = (t - 0.5f) / 0.25f;
+      r = 0.05f + 0.95f * f; g = 0.95f - 0.05f * f; b = 0.3f - 0.25f * f;
+    } else {
+      const float f = (t - 0.75f) / 0.25f;
+      r = 1.0f; g = 0.9f - 0.7f * f; b = 0.05f;
+    }
+    const uint8_t rgb[3] = {(uint8_t)(clamp01(r) * 255.0f), (uint8_t)(clamp01(g) * 255.0f),
+                            (uint8_t)(clamp01(b) * 255.0f)};
+    for (int row = 0; row < 4; ++row) {
+      uint8_t* o = out + 4 * (row * 256 + i);
+      o[0] = rgb[0]; o[1] = rgb[1]; o[2] = rgb[2]; o[3] = 255;
+    }
+  }
+  return LBM_OK;
+}
+
+// Jitter LUT, r8 [256][256]: the top byte of successive states of the LCG
+// s' = 1664525 s + 1013904223 from s = 0x9E3779B9 (src/main.cpp:565-573).
+extern "C" int lbm_jitter_lut(uint8_t* out) {
+  if (!out) return LBM_ERR_INVALID_ARG;
+  uint32_t s = 0x9E3779B9u;
+  for (int i = 0; i < 256 * 256; ++i) {
+    s = s * 1664525u + 1013904223u;
+    out[i] = (uint8_t)((s >> 24) & 0xFFu);
+  }
+  return LBM_OK;
+}
+

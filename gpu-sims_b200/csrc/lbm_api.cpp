@@ -515,6 +515,30 @@ int lbm_write_populations(lbm_ctx* c, const float* f, size_t n) {
   return LBM_OK;
 }
 
+int lbm_read_populations_shifted(lbm_ctx* c, float* g, size_t n) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!g || n != 19 * c->n) return fail(c, LBM_ERR_INVALID_ARG, "g must hold 19*Nx*Ny*Nz floats");
+  if (c->d.mode != LBM_MODE_PHYSICS) return fail(c, LBM_ERR_UNSUPPORTED, "shifted populations need physics mode");
+  if (!c->initialized) return fail(c, LBM_ERR_STATE, "read_populations_shifted before lbm_init_*");
+  if (int rc = ensure_staging(c, n * sizeof(float))) return rc;
+  CK(lbm::phys_read_pops(*c, static_cast<float*>(c->staging), c->stream, true), "gather populations");
+  CK(cudaMemcpyAsync(g, c->staging, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream), "read populations");
+  CK(cudaStreamSynchronize(c->stream), "read_populations_shifted sync");
+  return LBM_OK;
+}
+
+int lbm_write_populations_shifted(lbm_ctx* c, const float* g, size_t n) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!g || n != 19 * c->n) return fail(c, LBM_ERR_INVALID_ARG, "g must hold 19*Nx*Ny*Nz floats");
+  if (c->d.mode != LBM_MODE_PHYSICS) return fail(c, LBM_ERR_UNSUPPORTED, "shifted populations need physics mode");
+  if (int rc = ensure_staging(c, n * sizeof(float))) return rc;
+  CK(cudaMemcpyAsync(c->staging, g, n * sizeof(float), cudaMemcpyHostToDevice, c->stream), "write populations");
+  CK(lbm::phys_write_pops(*c, static_cast<const float*>(c->staging), c->stream, true), "scatter populations");
+  CK(cudaStreamSynchronize(c->stream), "write_populations_shifted sync");
+  c->initialized = true;
+  return LBM_OK;
+}
+
 int lbm_read_mask(lbm_ctx* c, uint8_t* mask, size_t n) {
   if (int rc = check_ctx(c)) return rc;
   if (!mask || n != c->n) return fail(c, LBM_ERR_INVALID_ARG, "mask must hold Nx*Ny*Nz bytes");

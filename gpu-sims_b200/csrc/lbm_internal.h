@@ -93,8 +93,10 @@ cudaError_t phys_step_bf16(const Ctx& c, int parity, bool write_moments, cudaStr
 cudaError_t phys_step_clo_f32(const Ctx& c, int parity, bool write_moments, cudaStream_t s);
 cudaError_t phys_step_clo_f16(const Ctx& c, int parity, bool write_moments, cudaStream_t s);
 cudaError_t phys_step_clo_bf16(const Ctx& c, int parity, bool write_moments, cudaStream_t s);
-cudaError_t phys_read_pops(const Ctx& c, float* out, cudaStream_t s);
-cudaError_t phys_write_pops(const Ctx& c, const float* in, cudaStream_t s);
+// Populations in natural layout [19][N]: f = g + w, or with `shifted` the
+// stored g = f - w itself (lossless for every storage precision).
+cudaError_t phys_read_pops(const Ctx& c, float* out, cudaStream_t s, bool shifted = false);
+cudaError_t phys_write_pops(const Ctx& c, const float* in, cudaStream_t s, bool shifted = false);
 
 // shared utilities (util_kernels.cu)
 cudaError_t classify(const Ctx& c, const int per[3], cudaStream_t s);

@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(256)
 template <int PREC>
 __global__ void __launch_bounds__(256)
     k_phys_read(PhysGeom G, int P, const void* __restrict__ pop_v, const uint8_t* __restrict__ flags,
-                float* __restrict__ out) {
+                float* __restrict__ out, int shifted) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z * blockDim.z + threadIdx.z;
@@ -121,14 +121,14 @@ __global__ void __launch_bounds__(256)
   fetch<PREC>(G, P, reinterpret_cast<const typename Store<PREC>::T*>(pop_v), x, y, z, g);
   static_for<0, Q>([&](auto I) {
     constexpr int i = decltype(I)::value;
-    out[(size_t)i * G.n + nid] = g[i] + wf(i);
+    out[(size_t)i * G.n + nid] = shifted ? g[i] : g[i] + wf(i);
   });
 }
 
 template <int PREC>
 __global__ void __launch_bounds__(256)
     k_phys_write(PhysGeom G, int P, void* __restrict__ pop_v, const uint8_t* __restrict__ flags,
-                 const float* __restrict__ in) {
+                 const float* __restrict__ in, int shifted) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z * blockDim.z + threadIdx.z;
@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(256)
   float g[Q];
   static_for<0, Q>([&](auto I) {
     constexpr int i = decltype(I)::value;
-    g[i] = in[(size_t)i * G.n + nid] - wf(i);
+    g[i] = shifted ? in[(size_t)i * G.n + nid] : in[(size_t)i * G.n + nid] - wf(i);
   });
   place<PREC>(G, P, reinterpret_cast<typename Store<PREC>::T*>(pop_v), x, y, z, g);
 }
@@ -192,32 +192,32 @@ cudaError_t phys_init(const Ctx& c, const float* rho, const float* u3, float rho
   return cudaGetLastError();
 }
 
-cudaError_t phys_read_pops(const Ctx& c, float* out, cudaStream_t s) {
+cudaError_t phys_read_pops(const Ctx& c, float* out, cudaStream_t s, bool shifted) {
   const PhysGeom& G = c.pp.g;
   switch (c.d.precision) {
     case LBM_PREC_F32:
-      k_phys_read<LBM_PREC_F32><<<phys_grid(G), phys_block(), 0, s>>>(G, c.parity, c.pop, c.flags, out);
+      k_phys_read<LBM_PREC_F32><<<phys_grid(G), phys_block(), 0, s>>>(G, c.parity, c.pop, c.flags, out, shifted ? 1 : 0);
       break;
     case LBM_PREC_F16S:
-      k_phys_read<LBM_PREC_F16S><<<phys_grid(G), phys_block(), 0, s>>>(G, c.parity, c.pop, c.flags, out);
+      k_phys_read<LBM_PREC_F16S><<<phys_grid(G), phys_block(), 0, s>>>(G, c.parity, c.pop, c.flags, out, shifted ? 1 : 0);
       break;
     default:
-      k_phys_read<LBM_PREC_BF16S><<<phys_grid(G), phys_block(), 0, s>>>(G, c.parity, c.pop, c.flags, out);
+      k_phys_read<LBM_PREC_BF16S><<<phys_grid(G), phys_block(), 0, s>>>(G, c.parity, c.pop, c.flags, out, shifted ? 1 : 0);
   }
   return cudaGetLastError();
 }
 
-cudaError_t phys_write_pops(const Ctx& c, const float* in, cudaStream_t s) {
+cudaError_t phys_write_pops(const Ctx& c, const float* in, cudaStream_t s, bool shifted) {
   const PhysGeom& G = c.pp.g;
   switch (c.d.precision) {
     case LBM_PREC_F32:
-      k_phys_write<LBM_PREC_F32><<<phys_grid(G), phys_block(), 0, s>>>(G, c.parity, c.pop, c.flags, in);
+      k_phys_write<LBM_PREC_F32><<<phys_grid(G), phys_block(), 0, s>>>(G, c.parity, c.pop, c.flags, in, shifted ? 1 : 0);
       break;
     case LBM_PREC_F16S:
-      k_phys_write<LBM_PREC_F16S><<<phys_grid(G), phys_block(), 0, s>>>(G, c.parity, c.pop, c.flags, in);
+      k_phys_write<LBM_PREC_F16S><<<phys_grid(G), phys_block(), 0, s>>>(G, c.parity, c.pop, c.flags, in, shifted ? 1 : 0);
       break;
     default:
-      k_phys_write<LBM_PREC_BF16S><<<phys_grid(G), phys_block(), 0, s>>>(G, c.parity, c.pop, c.flags, in);
+      k_phys_write<LBM_PREC_BF16S><<<phys_grid(G), phys_block(), 0, s>>>(G, c.parity, c.pop, c.flags, in, shifted ? 1 : 0);
   }
   return cudaGetLastError();
 }

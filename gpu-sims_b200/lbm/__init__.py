@@ -101,6 +101,15 @@ CAPTURE_LOAD_MASK = 1
 CAPTURE_MOMENTS_ONLY = 2
 
 
+class VelmagParams(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_uint32), ("inv_view_proj", C.c_float * 16), ("camera_pos", C.c_float * 3),
+        ("volume_min", C.c_float * 3), ("volume_max", C.c_float * 3), ("steps", C.c_int32),
+        ("absorption", C.c_float), ("velmag_min", C.c_float), ("velmag_max", C.c_float),
+        ("exposure", C.c_float), ("round_f16", C.c_int32),
+    ]
+
+
 class Adam(C.Structure):
     _fields_ = [
         ("struct_size", C.c_uint32), ("lr", C.c_float), ("beta1", C.c_float),
@@ -159,6 +168,8 @@ _SIGS = {
     "lbm_batch_get_info": (C.c_int, [_P, C.POINTER(BatchInfo)]),
     "lbm_batch_last_error": (C.c_char_p, [_P]),
     "lbm_read_mask": (C.c_int, [_P, _P, C.c_size_t]),
+    "lbm_read_populations_shifted": (C.c_int, [_P, _P, C.c_size_t]),
+    "lbm_write_populations_shifted": (C.c_int, [_P, _P, C.c_size_t]),
     "lbm_get_desc": (C.c_int, [_P, C.POINTER(Desc)]),
     "lbm_set_iteration": (C.c_int, [_P, _U64]),
     "lbm_capture_write": (C.c_int, [C.c_char_p, C.c_uint32, C.c_char_p, _I32, _I32, _I32, _P, _P, _P, _P]),
@@ -167,6 +178,13 @@ _SIGS = {
     "lbm_capture_save": (C.c_int, [_P, C.c_char_p, C.c_uint32, C.c_char_p, C.c_int]),
     "lbm_capture_load": (C.c_int, [_P, C.c_char_p, C.c_int]),
     "lbm_capture_last_error": (C.c_char_p, []),
+    "lbm_streamline_advect": (C.c_int, [_P, _I32, _I32, _I32, _P, C.c_uint32, C.c_uint32, C.c_uint32,
+                                        C.c_uint32, _F, C.c_uint32, _I32, _P]),
+    "lbm_streamline_seed": (C.c_int, [_P, C.c_uint32, C.c_uint32, _I32, _I32, _I32, C.c_uint32, C.c_uint32]),
+    "lbm_velmag_params_default": (C.c_int, [C.POINTER(VelmagParams)]),
+    "lbm_render_velmag": (C.c_int, [_P, _I32, _I32, _I32, C.POINTER(VelmagParams), _I32, _I32, _P, _P]),
+    "lbm_colormap_lut": (C.c_int, [_P]),
+    "lbm_jitter_lut": (C.c_int, [_P]),
     "lbm_set_closure": (C.c_int, [_P, _P]),
     "lbm_box_filter": (C.c_int, [_P, _P, _I32, _I32, _I32, _I32, _P, _P]),
     "lbm_closure_samples": (C.c_int, [_P, _I32, _I32, _I32, _F, _F, _U64, _I64, _P, _P, _P, _P]),
@@ -297,6 +315,15 @@ class Lattice:
     def set_flags(self, mask: np.ndarray) -> None:
         m = np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
         self._c(load().lbm_set_flags(self._h, _ptr(m), m.size))
+
+    def read_populations_shifted(self) -> np.ndarray:
+        g = np.empty((19, self.n), np.float32)
+        self._c(load().lbm_read_populations_shifted(self._h, _ptr(g), g.size))
+        return g
+
+    def write_populations_shifted(self, g: np.ndarray) -> None:
+        a = np.ascontiguousarray(g, dtype=np.float32)
+        self._c(load().lbm_write_populations_shifted(self._h, _ptr(a), a.size))
 
     def read_mask(self) -> np.ndarray:
         out = np.zeros(self.n, np.uint8)
@@ -674,3 +701,98 @@ def capture_latest(root: str) -> str:
     buf = C.create_string_buffer(4096)
     _cap_check(load().lbm_capture_latest(str(root).encode(), buf, 4096))
     return buf.value.decode()
+
+
+# ---- streamlines (include/lbm.h) -----------------------------------------------
+STREAMLINE_COUNT = 10000
+STREAMLINE_HISTORY = 64
+STREAMLINE_RESEED_AGE = 256
+STREAMLINE_SEED = 12345
+
+
+def streamline_seed(count: int, history: int, shape, seed: int = STREAMLINE_SEED,
+                    reseed_age: int = STREAMLINE_RESEED_AGE) -> np.ndarray:
+    """Host seeding of the position ring: float32 [count][history][4]."""
+    nx, ny, nz = shape
+    out = np.empty((count, history, 4), np.float32)
+    _check(load().lbm_streamline_seed(_ptr(out), count, history, nx, ny, nz, seed, reseed_age))
+    return out
+
+
+def streamline_advect(d_u: int, shape, d_positions: int, count: int, history: int, head: int,
+                      frame: int, dt_render: float, reseed_age: int = STREAMLINE_RESEED_AGE,
+                      round_f16: bool = True, stream=None) -> None:
+    """One advect pass over device positions (float4 ring)."""
+    nx, ny, nz = shape
+    _check(load().lbm_streamline_advect(d_u, nx, ny, nz, d_positions, count, history, head, frame,
+                                        dt_render, reseed_age, int(round_f16), stream))
+
+
+# ---- velocity-magnitude raymarch (include/lbm.h) --------------------------------
+
+def velmag_params(**kw) -> VelmagParams:
+    p = VelmagParams()
+    _check(load().lbm_velmag_params_default(C.byref(p)))
+    for k, v in kw.items():
+        if k in ("inv_view_proj", "camera_pos", "volume_min", "volume_max"):
+            arr = getattr(p, k)
+            vals = np.asarray(v, np.float32).reshape(-1)
+            for i in range(len(arr)):
+                arr[i] = float(vals[i])
+        else:
+            setattr(p, k, v)
+    return p
+
+
+def render_velmag(d_u: int, shape, params: VelmagParams, width: int, height: int, d_rgba: int,
+                  stream=None) -> None:
+    nx, ny, nz = shape
+    _check(load().lbm_render_velmag(d_u, nx, ny, nz, C.byref(params), width, height, d_rgba, stream))
+
+
+def colormap_lut() -> np.ndarray:
+    out = np.empty((4, 256, 4), np.uint8)
+    _check(load().lbm_colormap_lut(_ptr(out)))
+    return out
+
+
+def jitter_lut() -> np.ndarray:
+    out = np.empty((256, 256), np.uint8)
+    _check(load().lbm_jitter_lut(_ptr(out)))
+    return out
+
+
+def camera(eye, target, up=(0.0, 1.0, 0.0), fov_deg: float = 55.0, aspect: float = 16 / 9,
+           near: float = 0.05, far: float = 4000.0) -> np.ndarray:
+    """Inverse view-projection (column-major float[16]) of a right-handed
+    look-at camera with a [0, 1]-depth perspective, the conventions of glm's
+    lookAt and perspective under GLM_FORCE_DEPTH_ZERO_TO_ONE (the
+    reference's defaults: fov 55 deg, near 0.05, far 4000,
+    src/main.cpp:89-91)."""
+    e, t, u = (np.asarray(a, np.float64) for a in (eye, target, up))
+    f = (t - e) / np.linalg.norm(t - e)
+    s = np.cross(f, u)
+    s /= np.linalg.norm(s)
+    uu = np.cross(s, f)
+    view = np.eye(4)
+    view[0, :3], view[1, :3], view[2, :3] = s, uu, -f
+    view[0, 3], view[1, 3], view[2, 3] = -s @ e, -uu @ e, f @ e
+    th = np.tan(np.radians(fov_deg) / 2)
+    proj = np.zeros((4, 4))
+    proj[0, 0] = 1 / (aspect * th)
+    proj[1, 1] = 1 / th
+    proj[2, 2] = far / (near - far)
+    proj[3, 2] = -1.0
+    proj[2, 3] = -(far * near) / (far - near)
+    inv = np.linalg.inv(proj @ view)
+    return inv.T.reshape(-1).astype(np.float32)  # column-major
+
+
+def write_ppm(path: str, rgba: np.ndarray) -> None:
+    """Binary PPM of an RGBA float image [H][W][4] (colour over black,
+    clamped to [0, 1])."""
+    rgb = (np.clip(rgba[..., :3], 0.0, 1.0) * 255.0 + 0.5).astype(np.uint8)
+    h, w = rgb.shape[:2]
+    with open(path, "wb") as f:
+        f.write(f"P6 {w} {h} 255\n".encode())
+        f.write(rgb.tobytes())

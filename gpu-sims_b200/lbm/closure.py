@@ -307,7 +307,7 @@ def run(fine: int = 512, factor: int = 4, tau_f: float = 0.508, snapshots: int =
         every: int = 8, samples_per_snapshot: int = 4096, cs0: float = 0.1, seed: int = 5,
         u_rms: float = 0.04, epochs: int = 20, batch: int = 4096, lr: float = 1e-3,
         eval_every: int = 250, kmax: int = 16,
-        calibrate=(0.25, 0.5, 0.75, 1.0, 1.5, 2.0, 3.0, 4.0, 6.0), verbose: bool = True) -> dict:
+        calibrate=(0.1, 0.15, 0.2, 0.25, 0.35, 0.5, 0.75, 1.0, 1.5, 2.0), verbose: bool = True) -> dict:
     """The experiment: a training run (seed) gives the samples and, by a
     sweep of a single scale on Cs0 against its own filtered spectra, the
     calibration of the learned closure; a held-out run (seed + 1) is the

@@ -179,6 +179,11 @@ LBM_API int lbm_conservation(lbm_ctx* ctx, double out[4]);
  * post-collision populations of the current step.  For checkpoints. */
 LBM_API int lbm_read_populations(lbm_ctx* ctx, float* f, size_t n);
 LBM_API int lbm_write_populations(lbm_ctx* ctx, const float* f, size_t n);
+/* The same in physics mode as stored: g = f - w (fp32 values of the fp32,
+ * fp16-shifted or bf16-shifted store), which round-trips bit for bit (f does
+ * not: f - w + w is rounded).  Reference mode: LBM_ERR_UNSUPPORTED. */
+LBM_API int lbm_read_populations_shifted(lbm_ctx* ctx, float* g, size_t n);
+LBM_API int lbm_write_populations_shifted(lbm_ctx* ctx, const float* g, size_t n);
 
 LBM_API int lbm_get_info(lbm_ctx* ctx, lbm_info* info);
 
@@ -225,7 +230,8 @@ LBM_API int lbm_set_iteration(lbm_ctx* ctx, uint64_t iteration);
  *   velocity       rgba16f  uint16 half[N][4], w = 0
  *   obstacle_mask  r8uint   uint8[N], "frame_invariant": true
  *   populations    r32f     float[19][N], shape [19, Nx, Ny, Nz],
- *                           post-collision f (full-state
+ *                           post-collision f, or in physics mode f - w
+ *                           ("values": "f - w" in its entry) (full-state
  *                           checkpoint; not in the reference, which cannot
  *                           resume exactly, docs/tier1-capture-format-
  *                           reference.md:124-134)
@@ -270,6 +276,71 @@ LBM_API int lbm_capture_save(lbm_ctx* ctx, const char* root, uint32_t frame,
  * iteration counter from the meta. */
 LBM_API int lbm_capture_load(lbm_ctx* ctx, const char* dir, int flags);
 LBM_API const char* lbm_capture_last_error(void);
+
+/* ---- streamlines ------------------------------------------------------- */
+/* Streamline advection over the device velocity field, the reference's
+ * streamline_advect compute pass (shaders/streamline_advect.comp.glsl:34-91,
+ * dispatched from src/main.cpp:1596-1623) without the draw.  Positions are
+ * float4 (x, y, z, age) in lattice units, `history` per streamline in a
+ * ring (streamline s, slot h at s*history + h); domain [0, N] per axis.
+ * Per call and streamline: read slot (head_index - 1) mod history; if its
+ * age >= reseed_age or it left the domain, reseed it into the inlet slab
+ * x in [Nx/16, Nx/8] (xorshift32 seeded by s*2654435761 ^ frame*1597334677)
+ * and fill every slot; else take one RK2 step of dt_render with trilinear,
+ * clamp-to-edge velocity (texel centres at i + 1/2; fp32 with every
+ * operation rounded on its own; u rounded to binary16 first when round_f16,
+ * as the rgba16f image holds it) and write slot head_index.  The caller
+ * advances head_index = (head_index + 1) mod history after each call, as
+ * src/main.cpp:1621 does.  d_u: float[3][N] planes (lbm_device_moments);
+ * d_positions 16-byte aligned. */
+LBM_API int lbm_streamline_advect(const float* d_u, int32_t nx, int32_t ny, int32_t nz,
+                                  float* d_positions, uint32_t count, uint32_t history,
+                                  uint32_t head_index, uint32_t frame_count, float dt_render,
+                                  uint32_t reseed_age, int32_t round_f16, void* stream);
+/* Host seeding of the ring (src/main.cpp:1126-1152): std::mt19937(seed) and
+ * std::uniform_real_distribution<float>(0, 1); per streamline an initial age
+ * u*reseed_age, then x in [Nx/16, Nx/8], y in [0, Ny], z in [0, Nz]; every
+ * slot holds the seed.  The reference uses seed 12345, reseed_age 256,
+ * count 10000, history 64. */
+LBM_API int lbm_streamline_seed(float* positions, uint32_t count, uint32_t history,
+                                int32_t nx, int32_t ny, int32_t nz, uint32_t seed,
+                                uint32_t reseed_age);
+
+/* ---- velocity-magnitude raymarch ---------------------------------------- */
+/* The reference's velmag volume pass (shaders/velmag.frag.glsl:44-96, drawn
+ * by src/main.cpp:1720-1740) into a headless float RGBA buffer
+ * d_rgba[height][width][4] (row 0 at the top), no graphics API: per pixel a
+ * ray from camera_pos through the far-plane point of its fragment
+ * (inv_view_proj applied to ((px+1/2)/W*2-1, (py+1/2)/H*2-1, 1, 1)),
+ * clipped to the volume box, `steps` samples with blue-noise jitter (the
+ * reference's 256x256 LCG jitter LUT, src/main.cpp:565-573), |u| mapped to
+ * [velmag_min, velmag_max] and the colour LUT (src/main.cpp:529-563),
+ * front-to-back emission-absorption; alpha = 1 - transmittance.  Samplers,
+ * sqrt and exp are evaluated with separately rounded fp32 operations (see
+ * gpu-sims_b200/csrc/render.cu). */
+typedef struct lbm_velmag_params {
+    uint32_t struct_size;
+    float    inv_view_proj[16];   /* column-major, as glm::mat4 in memory   */
+    float    camera_pos[3];
+    float    volume_min[3];       /* default (0, 0, 0)                      */
+    float    volume_max[3];       /* default (-1, -1, -1) = (Nx, Ny, Nz)    */
+    int32_t  steps;               /* raymarchSteps, default 128             */
+    float    absorption;          /* velmagAbsorption, default 4            */
+    float    velmag_min;          /* default 0                              */
+    float    velmag_max;          /* default 0.1 (presets: 1.5 |u_inf|)     */
+    float    exposure;            /* default 1.5                            */
+    int32_t  round_f16;           /* sample u rounded to binary16 (rgba16f) */
+} lbm_velmag_params;
+
+LBM_API int lbm_velmag_params_default(lbm_velmag_params* p);
+LBM_API int lbm_render_velmag(const float* d_u, int32_t nx, int32_t ny, int32_t nz,
+                              const lbm_velmag_params* p, int32_t width, int32_t height,
+                              float* d_rgba, void* stream);
+/* The reference's LUTs (host): colour rgba8 [4][256][4] (build_colormap_lut,
+ * src/main.cpp:529-563) and jitter r8 [256][256] (build_jitter_lut,
+ * src/main.cpp:565-573). */
+LBM_API int lbm_colormap_lut(uint8_t* out);
+LBM_API int lbm_jitter_lut(uint8_t* out);
 
 /* ---- batched ensemble --------------------------------------------------- */
 /* Hundreds of independent physics-mode domains of uneven size advanced

@@ -39,6 +39,8 @@ def test_full_state_capture_resumes_exactly(gpu, tmp_path, mode, precision):
     assert np.array_equal(b.read_mask(), mask)
     assert b.info().iteration == 37
     assert np.array_equal(a.read_populations(), b.read_populations())
+    if mode == "physics":
+        assert np.array_equal(a.read_populations_shifted(), b.read_populations_shifted())
     a.step(25)
     b.step(25)
     assert np.array_equal(a.read_populations(), b.read_populations())
