@@ -12,6 +12,8 @@
 #pragma once
 #include <cstdint>
 
+#include <cuda_bf16.h>
+
 #include "fops.cuh"
 #include "lbm_internal.h"
 
@@ -28,6 +30,47 @@ template <> struct CloNet<2> {
   float v[CLO_FLOATS];
   __device__ __forceinline__ float operator[](int k) const { return v[k]; }
 };
+
+// SGS 3: the same network with its hidden layer on the tensor cores.  One
+// CTA of 128 threads, one node per thread, evaluates its 128 nodes' 32 x 32
+// hidden layer as one tcgen05 MMA (M = 128, N = 32, K = 32 in two K = 16
+// steps; bf16 operands in shared memory, fp32 accumulator in tensor memory):
+// each thread writes its node's first-layer activations (bf16) as row r of
+// A, thread 0 issues the MMAs, every thread reads its row of D back from
+// tensor memory (warp w owns TMEM lanes 32w .. 32w+31) and finishes the
+// output layer on CUDA cores.  The first layer (9 -> 32) stays on CUDA
+// cores.  Built by k_phys_step_tc (phys_step_launch.cuh), which owns the
+// shared tiles, the mbarrier and the TMEM columns.
+template <> struct CloNet<3> {
+  const CloNet<2>* net;     // parameters (kernel parameter space)
+  uint8_t* sA;              // A tile: 128 rows x 32 bf16, canonical K-major layout
+  uint32_t sA_addr, sB_addr, mbar_addr;  // shared-window addresses
+  uint32_t tmem;            // TMEM base (lane 0, first column)
+  unsigned* status;
+  bool row_ok;              // this thread's row exists (y < ny)
+  __device__ __forceinline__ float operator[](int k) const { return net->v[k]; }
+};
+
+// Shared-memory matrix descriptor of a K-major tile without swizzle: 8-row x
+// 16-byte core matrices, rows 16 B apart, K-adjacent core matrices `lbo`
+// bytes apart, M/N-adjacent ones `sbo` bytes apart (tcgen05 descriptor
+// format: start >> 4 in bits 0-13, lbo >> 4 in 16-29, sbo >> 4 in 32-45,
+// version 1 in 46-47, layout 0 = no swizzle in 61-63).
+__host__ __device__ constexpr uint64_t clo_smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)(lbo >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) |
+         (1ull << 46);
+}
+// Instruction descriptor of kind::f16: D f32 (bit 4), A and B bf16 (bits 7,
+// 10), both K-major, N >> 3 in bits 17-22, M >> 4 in bits 24-28.
+constexpr uint32_t CLO_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+// byte offset of element (row, k) in a canonical K-major tile of 32 columns
+__host__ __device__ constexpr uint32_t clo_tile_off(int row, int k) {
+  return (uint32_t)((row >> 3) * 512 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+// bound of the wait for the MMA: the kernel reports LBM_ERR_TIMEOUT past it
+#ifndef LBM_CLO_WAIT_LIMIT
+#define LBM_CLO_WAIT_LIMIT (1 << 22)
+#endif
 
 namespace {
 
@@ -85,6 +128,77 @@ __device__ __forceinline__ typename O::F closure_mlp(const W& w, const typename 
     z = O::fma(O::splat(w[CLO_W3 + i]), O::relu(a), z);
   }
   return O::softplus(z);
+}
+
+// The tensor-core evaluation of CloNet<3> (see there); every thread of the
+// CTA calls it once, with its own node's raw inputs.
+__device__ __forceinline__ float closure_mlp_tc(const CloNet<3>& c, const float (&xr)[CLO_IN]) {
+  const CloNet<2>& w = *c.net;
+  const int r = threadIdx.y * 32 + threadIdx.x;
+  float x[CLO_IN];
+#pragma unroll
+  for (int j = 0; j < CLO_IN; ++j) x[j] = __fmul_rn(__fsub_rn(xr[j], w.v[CLO_MEAN + j]), w.v[CLO_ISCALE + j]);
+  uint32_t hp[CLO_HID / 2];
+#pragma unroll
+  for (int i = 0; i < CLO_HID; i += 2) {
+    float a0 = w.v[CLO_B1 + i], a1 = w.v[CLO_B1 + i + 1];
+#pragma unroll
+    for (int j = 0; j < CLO_IN; ++j) {
+      a0 = __fmaf_rn(w.v[CLO_W1 + i * CLO_IN + j], x[j], a0);
+      a1 = __fmaf_rn(w.v[CLO_W1 + (i + 1) * CLO_IN + j], x[j], a1);
+    }
+    const __nv_bfloat162 h = __floats2bfloat162_rn(fmaxf(a0, 0.f), fmaxf(a1, 0.f));
+    hp[i / 2] = *reinterpret_cast<const uint32_t*>(&h);
+  }
+  uint8_t* row = c.sA + clo_tile_off(r, 0);
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+    *reinterpret_cast<uint4*>(row + q * 128) = make_uint4(hp[4 * q], hp[4 * q + 1], hp[4 * q + 2], hp[4 * q + 3]);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  __syncthreads();
+  if (r == 0) {
+#pragma unroll
+    for (int kk = 0; kk < 2; ++kk) {
+      const uint64_t da = clo_smem_desc(c.sA_addr + kk * 256, 128, 512);
+      const uint64_t db = clo_smem_desc(c.sB_addr + kk * 256, 128, 512);
+      asm volatile(
+          "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+          "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+          :: "r"(c.tmem), "l"(da), "l"(db), "r"(CLO_IDESC), "r"(kk) : "memory");
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 :: "r"(c.mbar_addr) : "memory");
+  }
+  uint32_t done = 0;
+  for (int it = 0; it < LBM_CLO_WAIT_LIMIT && !done; ++it)
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(done) : "r"(c.mbar_addr), "r"(0u) : "memory");
+  // the tensor-memory load below is warp-collective: decide per warp
+  if (!__all_sync(0xffffffffu, done != 0)) {  // gave up: plain Smagorinsky, error reported at sync
+    atomicOr(c.status, 2u);
+    return 1.0f;
+  }
+  __syncwarp();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  uint32_t v[CLO_HID];
+  const uint32_t ta = c.tmem + ((uint32_t)(threadIdx.y * 32) << 16);
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+        "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+        "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(ta));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+  float z = w.v[CLO_B3];
+#pragma unroll
+  for (int i = 0; i < CLO_HID; ++i)
+    z = __fmaf_rn(w.v[CLO_W3 + i], fmaxf(__fadd_rn(__uint_as_float(v[i]), w.v[CLO_B2 + i]), 0.f), z);
+  return Ops1::softplus(z);
 }
 
 }  // namespace

@@ -287,6 +287,25 @@ int lbm_set_stream(lbm_ctx* c, void* stream) {
   return LBM_OK;
 }
 
+int lbm_set_step_variant(lbm_ctx* c, int nodes_per_thread) {
+  if (int rc = check_ctx(c)) return rc;
+  const int v = nodes_per_thread;
+  if (v != 0 && v != 1 && v != 2 && v != 4) return fail(c, LBM_ERR_INVALID_ARG, "nodes_per_thread: 0, 1, 2 or 4");
+  if (c->d.mode != LBM_MODE_PHYSICS && v != 0)
+    return fail(c, LBM_ERR_UNSUPPORTED, "step variants are physics-mode kernels");
+  if (v == 2 && c->d.nx % 2) return fail(c, LBM_ERR_UNSUPPORTED, "two nodes per thread need an even nx");
+  if (v == 4 && (c->d.nx % 4 || c->d.precision == LBM_PREC_F32))
+    return fail(c, LBM_ERR_UNSUPPORTED, "four nodes per thread need nx % 4 == 0 and 2-byte storage");
+  CK(cudaStreamSynchronize(c->stream), "set_step_variant sync");
+  for (auto& g : c->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  c->step_variant = v;
+  return LBM_OK;
+}
+
 int lbm_set_closure(lbm_ctx* c, const float* net) {
   if (int rc = check_ctx(c)) return rc;
   if (c->d.mode != LBM_MODE_PHYSICS) return fail(c, LBM_ERR_UNSUPPORTED, "the closure needs physics mode");
@@ -442,6 +461,8 @@ int lbm_sync(lbm_ctx* c) {
   CK(cudaStreamSynchronize(c->stream), "sync");
   if (st) {
     CK(cudaMemsetAsync(c->status, 0, sizeof(unsigned), c->stream), "reset status");
+    if (st & 2u)
+      return fail(c, LBM_ERR_TIMEOUT, "the closure's tensor-core MMA wait gave up (nodes fell back to Smagorinsky)");
     return fail(c, LBM_ERR_NONFINITE, "non-finite value or rho <= 0 at a fluid node");
   }
   return LBM_OK;

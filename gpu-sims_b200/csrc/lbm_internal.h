@@ -139,6 +139,8 @@ struct Ctx {
   // value; weights already rounded to bf16
   bool closure = false;
   float clo[LBM_CLOSURE_FLOATS] = {};
+  // nodes per thread of the physics step: 0 automatic, 1, 2 or 4
+  int step_variant = 0;
   bool initialized = false;
   uint64_t iteration = 0;
   uint64_t dev_bytes = 0;

@@ -161,14 +161,15 @@ __device__ __forceinline__ void collide_t(const PhysParams& p, const CloNet<SGS>
     const F pn = O::mul(O::splat(INV), O::sqrt(q));
     const float cs2 = p.smag_cs * p.smag_cs;
     F k2 = O::splat(25.455844f * cs2);
-    if (SGS == 2) {
+    if constexpr (SGS >= 2) {
       // learned closure: Cs^2 = Cs0^2 r(features of Pi, rho)
       const F P[6] = {O::mul(O::splat(INV), pxx), O::mul(O::splat(INV), pyy),
                       O::mul(O::splat(INV), pzz), O::mul(O::splat(INV), pxy),
                       O::mul(O::splat(INV), pxz), O::mul(O::splat(INV), pyz)};
       F xin[CLO_IN];
       closure_features<O>(P, rho, xin);
-      k2 = O::mul(k2, closure_mlp<O>(net, xin));
+      if constexpr (SGS == 2) k2 = O::mul(k2, closure_mlp<O>(net, xin));
+      else k2 = O::mul(k2, closure_mlp_tc(net, xin));  // one node per thread (Ops1)
     }
     const F arg = O::fma(O::splat(p.tau), O::splat(p.tau), O::div(O::mul(k2, pn), rho));
     const F tau_eff = O::mul(O::splat(0.5f), O::add(O::splat(p.tau), O::sqrt(arg)));
@@ -320,8 +321,10 @@ __device__ __forceinline__ void step_row(const PhysParams& p, const CloNet<SGS>&
   const PhysGeom& G = p.g;
   const int lane = threadIdx.x & 31;
   const int x = x0 + lane;
-  const bool valid = x < G.nx;
-  const int xc = valid ? x : G.nx - 1;  // in-bounds address for idle lanes
+  bool row_ok = true;  // y < ny; only the tensor-core closure runs rows beyond
+  if constexpr (SGS == 3) row_ok = net.row_ok;
+  const bool valid = x < G.nx && row_ok;
+  const int xc = x < G.nx ? x : G.nx - 1;  // in-bounds address for idle lanes
   const bool edge = (lane == 31) || (x >= G.nx - 1);  // touches x+1 itself
   const uint32_t N = (uint32_t)G.n;
   const uint32_t nid = (uint32_t)xc + (uint32_t)G.nx * ((uint32_t)y + (uint32_t)G.ny * (uint32_t)z);
@@ -448,6 +451,18 @@ __host__ __device__ inline bool step_pairs(int nx) {
   if (nx % 2) return false;
   const int w64 = 64 * ((nx + 63) / 64), w32 = 32 * ((nx + 31) / 32);
   return 5 * w32 >= 4 * w64;
+#endif
+}
+
+// Four nodes per thread (step_row4, 2-byte formats) need nx % 4 == 0 and pay
+// off when the rows fill the 128-wide warps about as well as 64-wide ones.
+__host__ __device__ inline bool step_quads(int nx) {
+#ifdef LBM_NO_QUADS
+  return false;
+#else
+  if (nx % 4) return false;
+  const int w128 = 128 * ((nx + 127) / 128), w64 = 64 * ((nx + 63) / 64);
+  return 8 * w128 <= 9 * w64;
 #endif
 }
 
@@ -636,6 +651,231 @@ __device__ __forceinline__ void step_row2(const PhysParams& p, const CloNet<SGS>
         if (fluidA) S::raw_st(sP, i + 1, g2[a].x);
       }
       if (fluidB && edge) S::raw_st(sP, lnB + offs<1, DY, DZ>(G, wB), g2[a].y);
+    }
+  });
+}
+
+
+// Four x-adjacent 2-byte slots as one 8-byte access (x a multiple of 4).
+template <int PREC> struct Vec4;
+template <> struct Vec4<LBM_PREC_F16S> {
+  using T = __half;
+  static __device__ __forceinline__ uint2 ld(const T* p, uint32_t i) { return *reinterpret_cast<const uint2*>(p + i); }
+  static __device__ __forceinline__ float2 lo(uint2 v) { return __half22float2(*reinterpret_cast<const __half2*>(&v.x)); }
+  static __device__ __forceinline__ float2 hi(uint2 v) { return __half22float2(*reinterpret_cast<const __half2*>(&v.y)); }
+  static __device__ __forceinline__ uint32_t pack(float2 f) {
+    const __half2 h = __float22half2_rn(f);
+    return *reinterpret_cast<const uint32_t*>(&h);
+  }
+  static __device__ __forceinline__ void st(T* p, uint32_t i, float2 l, float2 h) {
+    *reinterpret_cast<uint2*>(p + i) = make_uint2(pack(l), pack(h));
+  }
+};
+template <> struct Vec4<LBM_PREC_BF16S> {
+  using T = __nv_bfloat16;
+  static __device__ __forceinline__ uint2 ld(const T* p, uint32_t i) { return *reinterpret_cast<const uint2*>(p + i); }
+  static __device__ __forceinline__ float2 lo(uint2 v) {
+    return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&v.x));
+  }
+  static __device__ __forceinline__ float2 hi(uint2 v) {
+    return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&v.y));
+  }
+  static __device__ __forceinline__ uint32_t pack(float2 f) {
+    const __nv_bfloat162 h = __float22bfloat162_rn(f);
+    return *reinterpret_cast<const uint32_t*>(&h);
+  }
+  static __device__ __forceinline__ void st(T* p, uint32_t i, float2 l, float2 h) {
+    *reinterpret_cast<uint2*>(p + i) = make_uint2(pack(l), pack(h));
+  }
+};
+
+// Four nodes per thread for the 2-byte formats (fp16 / bf16 shifted
+// storage), nx a multiple of 4: lane l updates x = x0 + 4l .. x + 3 (nodes A,
+// B, C, D); a warp covers 128 consecutive x.  The same scheme as step_row2
+// with 8-byte accesses: every slot quad moves as one access, the slots at
+// x+1 .. x+4 of the c_x = +1 pairs come from the lane's own vector and the
+// next lane's first element by one shuffle, the row's last quad touching
+// x+4 itself; A+B and C+D collide as two packed pairs (Ops2), so results are
+// bit-identical to the one- and two-node kernels.  Per node, the address,
+// flag and wall arithmetic is shared four ways instead of two, which is what
+// the issue-bound 2-byte kernel needs.
+template <int PREC, int COLL, int SGS, bool FORCE, bool WRITE_MOMENTS, int P>
+__device__ __forceinline__ void step_row4(const PhysParams& p, const CloNet<SGS>& net,
+                                          void* __restrict__ pop_v,
+                                          const uint8_t* __restrict__ flags,
+                                          const uint32_t* __restrict__ links,
+                                          float* __restrict__ rho_o, float* __restrict__ u_o,
+                                          unsigned* __restrict__ status, const int x0, const int y,
+                                          const int z) {
+  using S = Store<PREC>;
+  using V4 = Vec4<PREC>;
+  using T = typename S::T;
+  const PhysGeom& G = p.g;
+  const int lane = threadIdx.x & 31;
+  const int xa = x0 + 4 * lane;
+  const bool valid = xa < G.nx;
+  const int xc = valid ? xa : G.nx - 4;
+  const bool edge = (lane == 31) || (xa + 4 >= G.nx);  // its node D touches x+4 itself
+  const uint32_t N = (uint32_t)G.n;
+  const uint32_t nid = (uint32_t)xc + (uint32_t)G.nx * ((uint32_t)y + (uint32_t)G.ny * (uint32_t)z);
+  T* pop = reinterpret_cast<T*>(pop_v);
+  const size_t SS = G.slot_stride;
+  const uint32_t lnA = lin32(G, xc, y, z);
+  const uint32_t lnD = lnA + 3;
+  const Wrap w = wrap_terms(G, xc, y, z);       // y/z terms; nodes A..C never at x = nx-1
+  const Wrap wD = wrap_terms(G, xc + 3, y, z);  // x term of node D
+  const bool xloA = !G.per[0] && xc == 0, xhiD = !G.per[0] && xc + 3 == G.nx - 1;
+  const bool ylo = !G.per[1] && y == 0, yhi = !G.per[1] && y == G.ny - 1;
+  const bool zlo = !G.per[2] && z == 0, zhi = !G.per[2] && z == G.nz - 1;
+  const bool moving = p.any_moving_wall;
+
+  const uint32_t fl4 = valid ? *reinterpret_cast<const uint32_t*>(flags + nid) : 0x01010101u;
+  float2 gl[Q], gh[Q];  // gl: .x = A, .y = B;  gh: .x = C, .y = D
+  {
+    const uint2 r = V4::ld(pop, lnA);
+    gl[0] = V4::lo(r);
+    gh[0] = V4::hi(r);
+  }
+  static_for<0, 9>([&](auto PI) {
+    constexpr int pi = decltype(PI)::value;
+    constexpr int a = pair_a(pi), b = pair_b(pi);
+    constexpr int DX = cx(a), DY = cy(a), DZ = cz(a);
+    const T* s0 = pop + (size_t)(1 + 2 * pi) * SS;
+    const T* sP = P ? s0 + SS : s0;
+    const T* sQ = P ? s0 : s0 + SS;
+    const bool yz_fwd = (DY > 0 && yhi) || (DY < 0 && ylo) || (DZ > 0 && zhi) || (DZ < 0 && zlo);
+    const bool yz_bwd = (DY > 0 && ylo) || (DY < 0 && yhi) || (DZ > 0 && zlo) || (DZ < 0 && zhi);
+    // f_a of the four nodes from X = S[1-P](x..x+3); S[P] across a wall
+    const uint2 xv = V4::ld(yz_bwd ? sP : sQ, lnA);
+    gl[a] = V4::lo(xv);
+    gh[a] = V4::hi(xv);
+    if (DX > 0 && xloA) gl[a].x = S::raw_ld(sP, lnA);  // node A at the -x wall
+    // f_b from Y = S[P](n + d); S[1-P] across a wall
+    const uint2 yv = V4::ld(yz_fwd ? sQ : sP, lnA + offs<0, DY, DZ>(G, w));
+    const float2 ylo2 = V4::lo(yv), yhi2 = V4::hi(yv);
+    if (DX == 0) {
+      gl[b] = ylo2;
+      gh[b] = yhi2;
+    } else {
+      float nxt = __shfl_down_sync(FULL, ylo2.x, 1);  // x + 4
+      if (edge) nxt = S::raw_ld((yz_fwd || xhiD) ? sQ : sP, lnD + offs<1, DY, DZ>(G, wD));
+      gl[b] = make_float2(ylo2.y, yhi2.x);  // x + 1, x + 2
+      gh[b] = make_float2(yhi2.y, nxt);     // x + 3, x + 4
+    }
+  });
+  if (moving) {
+    static_for<0, 9>([&](auto PI) {
+      constexpr int pi = decltype(PI)::value;
+      constexpr int a = pair_a(pi), b = pair_b(pi);
+      constexpr int DX = cx(a), DY = cy(a), DZ = cz(a);
+      const bool yz_fwd = (DY > 0 && yhi) || (DY < 0 && ylo) || (DZ > 0 && zhi) || (DZ < 0 && zlo);
+      const bool yz_bwd = (DY > 0 && ylo) || (DY < 0 && yhi) || (DZ > 0 && zlo) || (DZ < 0 && zhi);
+      if (yz_bwd || (DX > 0 && xloA)) gl[a].x = fmaf(S::SC, wall_term<a>(p, xc, y, z), gl[a].x);
+      if (yz_bwd) {
+        gl[a].y = fmaf(S::SC, wall_term<a>(p, xc + 1, y, z), gl[a].y);
+        gh[a].x = fmaf(S::SC, wall_term<a>(p, xc + 2, y, z), gh[a].x);
+        gh[a].y = fmaf(S::SC, wall_term<a>(p, xc + 3, y, z), gh[a].y);
+      }
+      if (yz_fwd) {
+        gl[b].x = fmaf(S::SC, wall_term<b>(p, xc, y, z), gl[b].x);
+        gl[b].y = fmaf(S::SC, wall_term<b>(p, xc + 1, y, z), gl[b].y);
+        gh[b].x = fmaf(S::SC, wall_term<b>(p, xc + 2, y, z), gh[b].x);
+      }
+      if (yz_fwd || (DX > 0 && xhiD)) gh[b].y = fmaf(S::SC, wall_term<b>(p, xc + 3, y, z), gh[b].y);
+    });
+  }
+  const uint8_t fl[4] = {(uint8_t)(fl4 & 0xffu), (uint8_t)((fl4 >> 8) & 0xffu), (uint8_t)((fl4 >> 16) & 0xffu),
+                         (uint8_t)(fl4 >> 24)};
+  bool fluid[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) fluid[k] = valid && !(fl[k] & FLAG_SOLID);
+  // links into interior solids, per node (rare)
+  auto solid_fix = [&](auto kk, const Wrap& wn, bool xlo, bool xhi) {
+    constexpr int k = decltype(kk)::value;
+    auto at = [&](int i) -> float& {
+      return k == 0 ? gl[i].x : (k == 1 ? gl[i].y : (k == 2 ? gh[i].x : gh[i].y));
+    };
+    const uint32_t L = links[nid + k];
+    const uint32_t ln = lnA + k;
+    static_for<0, 9>([&](auto PI) {
+      constexpr int pi = decltype(PI)::value;
+      constexpr int a = pair_a(pi), b = pair_b(pi);
+      constexpr int DX = cx(a), DY = cy(a), DZ = cz(a);
+      const T* s0 = pop + (size_t)(1 + 2 * pi) * SS;
+      const T* sP = P ? s0 + SS : s0;
+      const T* sQ = P ? s0 : s0 + SS;
+      const bool fwd_wall = (DX > 0 && xhi) || (DY > 0 && yhi) || (DY < 0 && ylo) || (DZ > 0 && zhi) ||
+                            (DZ < 0 && zlo);
+      const bool bwd_wall =
+          (DX > 0 && xlo) || (DY > 0 && ylo) || (DY < 0 && yhi) || (DZ > 0 && zlo) || (DZ < 0 && zhi);
+      if (((L >> b) & 1u) && !bwd_wall) at(a) = S::raw_ld(sP, ln);
+      if (((L >> a) & 1u) && !fwd_wall) at(b) = S::raw_ld(sQ, ln + offs<DX, DY, DZ>(G, wn));
+    });
+  };
+  if (fluid[0] && (fl[0] & FLAG_SOLID_LINK)) solid_fix(IC<0>{}, w, xloA, false);
+  if (fluid[1] && (fl[1] & FLAG_SOLID_LINK)) solid_fix(IC<1>{}, w, false, false);
+  if (fluid[2] && (fl[2] & FLAG_SOLID_LINK)) solid_fix(IC<2>{}, w, false, false);
+  if (fluid[3] && (fl[3] & FLAG_SOLID_LINK)) solid_fix(IC<3>{}, wD, false, xhiD);
+
+  float2 rl, uxl, uyl, uzl, rh, uxh, uyh, uzh;
+  collide_t<Ops2, COLL, SGS, FORCE, PREC>(p, net, gl, rl, uxl, uyl, uzl);
+  collide_t<Ops2, COLL, SGS, FORCE, PREC>(p, net, gh, rh, uxh, uyh, uzh);
+
+  if (WRITE_MOMENTS && valid) {
+    auto m4 = [&](float* dst, float2 l, float2 h) {
+      *reinterpret_cast<float4*>(dst) = make_float4(fluid[0] ? l.x : 0.f, fluid[1] ? l.y : 0.f,
+                                                    fluid[2] ? h.x : 0.f, fluid[3] ? h.y : 0.f);
+    };
+    m4(rho_o + nid, rl, rh);
+    m4(u_o + nid, uxl, uxh);
+    m4(u_o + N + nid, uyl, uyh);
+    m4(u_o + 2 * N + nid, uzl, uzh);
+    auto bad = [](bool f, float r, float ux, float uy, float uz) {
+      return f && (!(r > 0.f) || !isfinite(r) || !isfinite(ux) || !isfinite(uy) || !isfinite(uz));
+    };
+    if (bad(fluid[0], rl.x, uxl.x, uyl.x, uzl.x) || bad(fluid[1], rl.y, uxl.y, uyl.y, uzl.y) ||
+        bad(fluid[2], rh.x, uxh.x, uyh.x, uzh.x) || bad(fluid[3], rh.y, uxh.y, uyh.y, uzh.y))
+      atomicOr(status, 1u);
+  }
+
+  const bool all4 = fluid[0] && fluid[1] && fluid[2] && fluid[3];
+  // store the four nodes' values at slot positions i .. i+3
+  auto st4 = [&](T* arr, uint32_t i, float2 l, float2 h) {
+    if (all4) V4::st(arr, i, l, h);
+    else {
+      if (fluid[0]) S::raw_st(arr, i, l.x);
+      if (fluid[1]) S::raw_st(arr, i + 1, l.y);
+      if (fluid[2]) S::raw_st(arr, i + 2, h.x);
+      if (fluid[3]) S::raw_st(arr, i + 3, h.y);
+    }
+  };
+  st4(pop, lnA, gl[0], gh[0]);
+  const bool passD = fluid[3] && !edge;  // node D's Y value at x+4 is stored by lane+1
+  static_for<0, 9>([&](auto PI) {
+    constexpr int pi = decltype(PI)::value;
+    constexpr int a = pair_a(pi), b = pair_b(pi);
+    constexpr int DX = cx(a), DY = cy(a), DZ = cz(a);
+    T* s0 = pop + (size_t)(1 + 2 * pi) * SS;
+    T* sP = P ? s0 + SS : s0;
+    T* sQ = P ? s0 : s0 + SS;
+    st4(sQ, lnA, gl[b], gh[b]);  // f*_b -> X = S[1-P](n)
+    if (DX == 0) {
+      st4(sP, lnA + offs<0, DY, DZ>(G, w), gl[a], gh[a]);  // f*_a -> Y = S[P](n+d)
+    } else {
+      // aligned quad (x .. x+3) of row (y+dy, z+dz): x from lane-1's node D,
+      // x+1 .. x+3 from nodes A, B, C
+      const float from_left = __shfl_up_sync(FULL, gh[a].y, 1);
+      const bool left_ok = __shfl_up_sync(FULL, passD, 1) && lane > 0;
+      const uint32_t i = lnA + offs<0, DY, DZ>(G, w);
+      if (left_ok && fluid[0] && fluid[1] && fluid[2]) {
+        V4::st(sP, i, make_float2(from_left, gl[a].x), make_float2(gl[a].y, gh[a].x));
+      } else {
+        if (left_ok) S::raw_st(sP, i, from_left);
+        if (fluid[0]) S::raw_st(sP, i + 1, gl[a].x);
+        if (fluid[1]) S::raw_st(sP, i + 2, gl[a].y);
+        if (fluid[2]) S::raw_st(sP, i + 3, gh[a].x);
+      }
+      if (fluid[3] && edge) S::raw_st(sP, lnD + offs<1, DY, DZ>(G, wD), gh[a].y);
     }
   });
 }

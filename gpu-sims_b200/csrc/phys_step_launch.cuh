@@ -45,6 +45,77 @@ __global__ void __launch_bounds__(STEP_THREADS, SGS == 2 ? LBM_CLO_MINB : LBM_ST
                                                      status, blockIdx.x * 32, y, blockIdx.z);
 }
 
+#ifndef LBM_STEP4_MINB
+#define LBM_STEP4_MINB 3
+#endif
+
+// Four nodes per thread (2-byte storage, nx % 4 == 0): a warp covers 128 x.
+template <int PREC, int COLL, int SGS, bool FORCE, bool WRITE_MOMENTS, int P>
+__global__ void __launch_bounds__(STEP_THREADS, LBM_STEP4_MINB)
+    k_phys_step4(PhysParams p, void* __restrict__ pop_v, const uint8_t* __restrict__ flags,
+                 const uint32_t* __restrict__ links, float* __restrict__ rho_o,
+                 float* __restrict__ u_o, unsigned* __restrict__ status,
+                 const __grid_constant__ CloNet<SGS> net) {
+  const int y = blockIdx.y * STEP_BY + threadIdx.y;
+  if (y >= p.g.ny) return;  // uniform over the warp
+  step_row4<PREC, COLL, SGS, FORCE, WRITE_MOMENTS, P>(p, net, pop_v, flags, links, rho_o, u_o,
+                                                      status, blockIdx.x * 128, y, blockIdx.z);
+}
+
+// Learned closure with the hidden layer on the tensor cores (CloNet<3>): one
+// node per thread, a CTA of 128 threads is one M = 128 MMA.  The CTA owns a
+// 32-column TMEM allocation, the bf16 A and B tiles and one mbarrier; rows
+// beyond ny run on the last row without storing, so every thread reaches the
+// CTA-wide barriers.
+template <int PREC, int COLL, bool WRITE_MOMENTS, int P>
+__global__ void __launch_bounds__(STEP_THREADS, LBM_CLO_MINB)
+    k_phys_step_tc(PhysParams p, void* __restrict__ pop_v, const uint8_t* __restrict__ flags,
+                   const uint32_t* __restrict__ links, float* __restrict__ rho_o,
+                   float* __restrict__ u_o, unsigned* __restrict__ status,
+                   const __grid_constant__ CloNet<2> net) {
+  static_assert(STEP_THREADS == 128, "one MMA row per thread");
+  __shared__ __align__(1024) uint8_t sA[128 * 64];
+  __shared__ __align__(1024) uint8_t sB[CLO_HID * 64];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tslot;
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  for (int e = tid; e < CLO_HID * CLO_HID; e += STEP_THREADS)
+    *reinterpret_cast<__nv_bfloat16*>(sB + clo_tile_off(e / CLO_HID, e % CLO_HID)) =
+        __float2bfloat16_rn(net.v[CLO_W2 + e]);
+  const uint32_t mbar_addr = (uint32_t)__cvta_generic_to_shared(&mbar);
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(mbar_addr), "r"(1) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (threadIdx.y == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"((uint32_t)__cvta_generic_to_shared(&tslot)), "r"(32) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const int y = blockIdx.y * STEP_BY + threadIdx.y;
+  CloNet<3> c;
+  c.net = &net;
+  c.sA = sA;
+  c.sA_addr = (uint32_t)__cvta_generic_to_shared(sA);
+  c.sB_addr = (uint32_t)__cvta_generic_to_shared(sB);
+  c.mbar_addr = mbar_addr;
+  c.tmem = tslot;
+  c.status = status;
+  c.row_ok = y < p.g.ny;
+  step_row<PREC, COLL, 3, false, WRITE_MOMENTS, P>(p, c, pop_v, flags, links, rho_o, u_o, status,
+                                                   blockIdx.x * 32, c.row_ok ? y : p.g.ny - 1,
+                                                   blockIdx.z);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (threadIdx.y == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(c.tmem), "r"(32) : "memory");
+  }
+}
+
 template <int SGS> CloNet<SGS> net_of(const Ctx&) { return CloNet<SGS>{}; }
 template <> CloNet<2> net_of<2>(const Ctx& c) {
   CloNet<2> n;
@@ -52,12 +123,41 @@ template <> CloNet<2> net_of<2>(const Ctx& c) {
   return n;
 }
 
+// Nodes per thread: the context's choice (lbm_set_step_variant) or, by
+// default, four for the 2-byte formats when step_quads(nx), two when
+// step_pairs(nx), else one.
+inline bool use_quads(const Ctx& c) {
+  const int nx = c.pp.g.nx;
+  if (c.d.precision == LBM_PREC_F32 || c.closure || nx % 4) return false;
+  return c.step_variant == 4 || (c.step_variant == 0 && step_quads(nx));
+}
+inline bool use_pairs(const Ctx& c) {
+  const int nx = c.pp.g.nx;
+  if (nx % 2 || c.step_variant == 1) return false;
+  return c.step_variant == 2 || c.step_variant == 4 || step_pairs(nx);
+}
+
 template <int PREC, int COLL, int SGS, bool FORCE>
 cudaError_t launch_step(const Ctx& c, int P, bool wm, cudaStream_t s) {
   const PhysGeom& G = c.pp.g;
   const CloNet<SGS> net = net_of<SGS>(c);
   const dim3 blk(32, STEP_BY, 1);
-  if (step_pairs(G.nx)) {
+  if constexpr (PREC != LBM_PREC_F32 && SGS != 2) {
+    if (use_quads(c)) {
+      const dim3 grd((G.nx + 127) / 128, (G.ny + STEP_BY - 1) / STEP_BY, G.nz);
+#define LBM_STEP_LAUNCH(WM, PAR)                                          \
+  k_phys_step4<PREC, COLL, SGS, FORCE, WM, PAR><<<grd, blk, 0, s>>>(      \
+      c.pp, c.pop, c.flags, c.links, c.rho, c.u, c.status, net)
+      if (wm) {
+        if (P) LBM_STEP_LAUNCH(true, 1); else LBM_STEP_LAUNCH(true, 0);
+      } else {
+        if (P) LBM_STEP_LAUNCH(false, 1); else LBM_STEP_LAUNCH(false, 0);
+      }
+#undef LBM_STEP_LAUNCH
+      return cudaGetLastError();
+    }
+  }
+  if (use_pairs(c)) {
     const dim3 grd((G.nx + 63) / 64, (G.ny + STEP_BY - 1) / STEP_BY, G.nz);
 #define LBM_STEP_LAUNCH(WM, PAR)                                          \
   k_phys_step2<PREC, COLL, SGS, FORCE, WM, PAR><<<grd, blk, 0, s>>>(      \
@@ -90,11 +190,31 @@ cudaError_t dispatch_force(const Ctx& c, int P, bool wm, cudaStream_t s) {
                : launch_step<PREC, COLL, SGS, false>(c, P, wm, s);
 }
 
+template <int PREC, int COLL>
+cudaError_t launch_step_tc(const Ctx& c, int P, bool wm, cudaStream_t s) {
+  const PhysGeom& G = c.pp.g;
+  const CloNet<2> net = net_of<2>(c);
+  const dim3 blk(32, STEP_BY, 1);
+  const dim3 grd((G.nx + 31) / 32, (G.ny + STEP_BY - 1) / STEP_BY, G.nz);
+#define LBM_STEP_LAUNCH(WM, PAR)                                          \
+  k_phys_step_tc<PREC, COLL, WM, PAR><<<grd, blk, 0, s>>>(                \
+      c.pp, c.pop, c.flags, c.links, c.rho, c.u, c.status, net)
+  if (wm) {
+    if (P) LBM_STEP_LAUNCH(true, 1); else LBM_STEP_LAUNCH(true, 0);
+  } else {
+    if (P) LBM_STEP_LAUNCH(false, 1); else LBM_STEP_LAUNCH(false, 0);
+  }
+#undef LBM_STEP_LAUNCH
+  return cudaGetLastError();
+}
+
 // CLOSURE: the learned-closure kernels (compiled in their own files; no body
-// force, which lbm_set_closure enforces).
+// force, which lbm_set_closure enforces): the tensor-core MLP by default,
+// the CUDA-core MLP for an explicit one- or two-node variant.
 template <int PREC, int COLL, bool CLOSURE>
 cudaError_t dispatch_smag(const Ctx& c, int P, bool wm, cudaStream_t s) {
   if constexpr (CLOSURE) {
+    if (c.step_variant == 0) return launch_step_tc<PREC, COLL>(c, P, wm, s);
     return launch_step<PREC, COLL, 2, false>(c, P, wm, s);
   } else {
     return c.pp.smag_cs > 0.f ? dispatch_force<PREC, COLL, 1>(c, P, wm, s)

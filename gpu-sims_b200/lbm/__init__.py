@@ -168,6 +168,7 @@ _SIGS = {
     "lbm_batch_get_info": (C.c_int, [_P, C.POINTER(BatchInfo)]),
     "lbm_batch_last_error": (C.c_char_p, [_P]),
     "lbm_read_mask": (C.c_int, [_P, _P, C.c_size_t]),
+    "lbm_set_step_variant": (C.c_int, [_P, C.c_int]),
     "lbm_read_populations_shifted": (C.c_int, [_P, _P, C.c_size_t]),
     "lbm_write_populations_shifted": (C.c_int, [_P, _P, C.c_size_t]),
     "lbm_get_desc": (C.c_int, [_P, C.POINTER(Desc)]),
@@ -324,6 +325,9 @@ class Lattice:
     def write_populations_shifted(self, g: np.ndarray) -> None:
         a = np.ascontiguousarray(g, dtype=np.float32)
         self._c(load().lbm_write_populations_shifted(self._h, _ptr(a), a.size))
+
+    def set_step_variant(self, nodes_per_thread: int) -> None:
+        self._c(load().lbm_set_step_variant(self._h, nodes_per_thread))
 
     def read_mask(self) -> np.ndarray:
         out = np.zeros(self.n, np.uint8)

@@ -156,8 +156,17 @@ LBM_API int lbm_init_from_moments(lbm_ctx* ctx, const float* rho, const void* u,
  * The moments of the last step are written for readback. */
 LBM_API int lbm_step(lbm_ctx* ctx, int nsteps);
 
+/* Physics mode: nodes per thread of the step kernel, 0 = automatic (four for
+ * fp16/bf16 storage when nx % 4 == 0 and the rows fill 128-wide warps, two
+ * when nx is even and the rows fill 64-wide warps, else one), or 1, 2, 4.
+ * All variants give bit-identical results; this is a tuning and testing
+ * knob.  LBM_ERR_UNSUPPORTED for a variant the grid or precision cannot use. */
+LBM_API int lbm_set_step_variant(lbm_ctx* ctx, int nodes_per_thread);
+
 /* Waits for the context's stream; returns LBM_ERR_NONFINITE if a NaN/Inf or
- * non-positive density was seen at a fluid node since the last sync. */
+ * non-positive density was seen at a fluid node since the last sync, and
+ * LBM_ERR_TIMEOUT if a learned-closure step's bounded wait for its
+ * tensor-core MMA gave up (those nodes used plain Smagorinsky). */
 LBM_API int lbm_sync(lbm_ctx* ctx);
 
 /* Copies rho (float[N]) and u (format u_fmt) to host memory; either pointer

@@ -317,3 +317,26 @@ def test_network_beats_constant_a_priori(gpu):
     ev.free()
     torch.cuda.set_stream(torch.cuda.default_stream())
     assert l_net < 0.97 * l_const and l_const <= l_smag, (l_net, l_const, l_smag)
+
+
+@pytest.mark.parametrize("shape", [(32, 12, 10), (40, 9, 6)])
+def test_tensor_core_mlp_matches_cuda_core_mlp(gpu, oracle, shape):
+    """The default closure step evaluates the hidden layer with tcgen05 MMAs
+    (bf16 activations); the CUDA-core variant keeps fp32 activations.  Both
+    agree with the FP64 ExtStep closure at the physics-mode bar (3e-5 of the
+    velocity scale) and with each other; ny not a multiple of the CTA's four
+    rows exercises the rows that only take part in the MMA."""
+    net = _net(13)
+    runs = []
+    for variant in (0, 1):
+        lat, st = _closure_pair(gpu, oracle, shape, net)
+        lat.set_step_variant(variant)
+        lat.step(40)
+        lat.sync()
+        runs.append(lat.read_moments()[1])
+        lat.close()
+    st.step(40)
+    scale = np.abs(st.u).max()
+    for u in runs:
+        assert np.max(np.abs(u.T - st.u)) / scale <= 3e-5
+    assert np.max(np.abs(runs[0] - runs[1])) / scale <= 3e-5
