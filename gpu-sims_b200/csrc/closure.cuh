@@ -48,6 +48,7 @@ template <> struct CloNet<3> {
   uint32_t tmem;            // TMEM base (lane 0, first column)
   unsigned* status;
   bool row_ok;              // this thread's row exists (y < ny)
+  uint32_t phase;           // mbarrier phase of this evaluation (alternates per use)
   __device__ __forceinline__ float operator[](int k) const { return net->v[k]; }
 };
 
@@ -154,8 +155,12 @@ __device__ __forceinline__ float closure_mlp_tc(const CloNet<3>& c, const float 
 #pragma unroll
   for (int q = 0; q < 4; ++q)
     *reinterpret_cast<uint4*>(row + q * 128) = make_uint4(hp[4 * q], hp[4 * q + 1], hp[4 * q + 2], hp[4 * q + 3]);
+  // the A tile is visible to the tensor core, and every thread has finished
+  // reading the previous evaluation's D, before the MMAs are issued
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (r == 0) {
 #pragma unroll
     for (int kk = 0; kk < 2; ++kk) {
@@ -174,7 +179,7 @@ __device__ __forceinline__ float closure_mlp_tc(const CloNet<3>& c, const float 
     asm volatile(
         "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
         "selp.b32 %0, 1, 0, P1;\n\t}\n"
-        : "=r"(done) : "r"(c.mbar_addr), "r"(0u) : "memory");
+        : "=r"(done) : "r"(c.mbar_addr), "r"(c.phase) : "memory");
   // the tensor-memory load below is warp-collective: decide per warp
   if (!__all_sync(0xffffffffu, done != 0)) {  // gave up: plain Smagorinsky, error reported at sync
     atomicOr(c.status, 2u);

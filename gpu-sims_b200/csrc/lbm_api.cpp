@@ -290,7 +290,8 @@ int lbm_set_stream(lbm_ctx* c, void* stream) {
 int lbm_set_step_variant(lbm_ctx* c, int nodes_per_thread) {
   if (int rc = check_ctx(c)) return rc;
   const int v = nodes_per_thread;
-  if (v != 0 && v != 1 && v != 2 && v != 4) return fail(c, LBM_ERR_INVALID_ARG, "nodes_per_thread: 0, 1, 2 or 4");
+  if (v != 0 && v != 1 && v != 2 && v != 4 && v != 8)
+    return fail(c, LBM_ERR_INVALID_ARG, "variant: 0, 1, 2, 4 or 8");
   if (c->d.mode != LBM_MODE_PHYSICS && v != 0)
     return fail(c, LBM_ERR_UNSUPPORTED, "step variants are physics-mode kernels");
   if (v == 2 && c->d.nx % 2) return fail(c, LBM_ERR_UNSUPPORTED, "two nodes per thread need an even nx");

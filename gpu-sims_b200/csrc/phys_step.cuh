@@ -454,15 +454,17 @@ __host__ __device__ inline bool step_pairs(int nx) {
 #endif
 }
 
-// Four nodes per thread (step_row4, 2-byte formats) need nx % 4 == 0 and pay
-// off when the rows fill the 128-wide warps about as well as 64-wide ones.
+// Four nodes per thread (step_row4, 2-byte formats) need nx % 4 == 0.  They
+// are not chosen automatically: measured on B200 on the 512 x 128 x 128
+// channel, fp16 runs at 46.8 GLUPS with four nodes per thread (167 registers,
+// three 128-thread blocks per SM) against 50.2 with two, so the automatic
+// choice stays at two; lbm_set_step_variant(ctx, 4) selects them.
 __host__ __device__ inline bool step_quads(int nx) {
-#ifdef LBM_NO_QUADS
-  return false;
+#ifdef LBM_AUTO_QUADS
+  return nx % 4 == 0;
 #else
-  if (nx % 4) return false;
-  const int w128 = 128 * ((nx + 127) / 128), w64 = 64 * ((nx + 63) / 64);
-  return 8 * w128 <= 9 * w64;
+  (void)nx;
+  return false;
 #endif
 }
 

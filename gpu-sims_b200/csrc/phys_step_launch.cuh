@@ -63,10 +63,14 @@ __global__ void __launch_bounds__(STEP_THREADS, LBM_STEP4_MINB)
 }
 
 // Learned closure with the hidden layer on the tensor cores (CloNet<3>): one
-// node per thread, a CTA of 128 threads is one M = 128 MMA.  The CTA owns a
-// 32-column TMEM allocation, the bf16 A and B tiles and one mbarrier; rows
+// node per thread, a CTA of 128 threads is one M = 128 MMA per z-plane, and
+// walks LBM_TC_ZPB planes so that its set-up (the 32-column TMEM allocation,
+// the bf16 W2 tile, the mbarrier) is paid once per several MMAs.  Rows
 // beyond ny run on the last row without storing, so every thread reaches the
 // CTA-wide barriers.
+#ifndef LBM_TC_ZPB
+#define LBM_TC_ZPB 8
+#endif
 template <int PREC, int COLL, bool WRITE_MOMENTS, int P>
 __global__ void __launch_bounds__(STEP_THREADS, LBM_CLO_MINB)
     k_phys_step_tc(PhysParams p, void* __restrict__ pop_v, const uint8_t* __restrict__ flags,
@@ -105,9 +109,13 @@ __global__ void __launch_bounds__(STEP_THREADS, LBM_CLO_MINB)
   c.tmem = tslot;
   c.status = status;
   c.row_ok = y < p.g.ny;
-  step_row<PREC, COLL, 3, false, WRITE_MOMENTS, P>(p, c, pop_v, flags, links, rho_o, u_o, status,
-                                                   blockIdx.x * 32, c.row_ok ? y : p.g.ny - 1,
-                                                   blockIdx.z);
+  const int z0 = blockIdx.z * LBM_TC_ZPB;
+  const int z1 = min(p.g.nz, z0 + LBM_TC_ZPB);  // uniform over the CTA
+  for (int z = z0; z < z1; ++z) {
+    c.phase = (uint32_t)((z - z0) & 1);
+    step_row<PREC, COLL, 3, false, WRITE_MOMENTS, P>(p, c, pop_v, flags, links, rho_o, u_o, status,
+                                                     blockIdx.x * 32, c.row_ok ? y : p.g.ny - 1, z);
+  }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (threadIdx.y == 0) {
@@ -133,7 +141,7 @@ inline bool use_quads(const Ctx& c) {
 }
 inline bool use_pairs(const Ctx& c) {
   const int nx = c.pp.g.nx;
-  if (nx % 2 || c.step_variant == 1) return false;
+  if (nx % 2 || c.step_variant == 1 || c.step_variant == 8) return false;
   return c.step_variant == 2 || c.step_variant == 4 || step_pairs(nx);
 }
 
@@ -195,7 +203,7 @@ cudaError_t launch_step_tc(const Ctx& c, int P, bool wm, cudaStream_t s) {
   const PhysGeom& G = c.pp.g;
   const CloNet<2> net = net_of<2>(c);
   const dim3 blk(32, STEP_BY, 1);
-  const dim3 grd((G.nx + 31) / 32, (G.ny + STEP_BY - 1) / STEP_BY, G.nz);
+  const dim3 grd((G.nx + 31) / 32, (G.ny + STEP_BY - 1) / STEP_BY, (G.nz + LBM_TC_ZPB - 1) / LBM_TC_ZPB);
 #define LBM_STEP_LAUNCH(WM, PAR)                                          \
   k_phys_step_tc<PREC, COLL, WM, PAR><<<grd, blk, 0, s>>>(                \
       c.pp, c.pop, c.flags, c.links, c.rho, c.u, c.status, net)
@@ -209,12 +217,15 @@ cudaError_t launch_step_tc(const Ctx& c, int P, bool wm, cudaStream_t s) {
 }
 
 // CLOSURE: the learned-closure kernels (compiled in their own files; no body
-// force, which lbm_set_closure enforces): the tensor-core MLP by default,
-// the CUDA-core MLP for an explicit one- or two-node variant.
+// force, which lbm_set_closure enforces): the CUDA-core MLP (one or two
+// nodes per thread) by default, the tensor-core MLP for variant 8.  Measured
+// on B200 at 128^3 the CUDA-core pair kernel runs 10.4 GLUPS and the
+// tensor-core kernel 8.9: its per-plane CTA barrier around the MMA leaves the
+// memory latency of the next plane exposed.
 template <int PREC, int COLL, bool CLOSURE>
 cudaError_t dispatch_smag(const Ctx& c, int P, bool wm, cudaStream_t s) {
   if constexpr (CLOSURE) {
-    if (c.step_variant == 0) return launch_step_tc<PREC, COLL>(c, P, wm, s);
+    if (c.step_variant == 8) return launch_step_tc<PREC, COLL>(c, P, wm, s);
     return launch_step<PREC, COLL, 2, false>(c, P, wm, s);
   } else {
     return c.pp.smag_cs > 0.f ? dispatch_force<PREC, COLL, 1>(c, P, wm, s)

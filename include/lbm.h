@@ -156,11 +156,14 @@ LBM_API int lbm_init_from_moments(lbm_ctx* ctx, const float* rho, const void* u,
  * The moments of the last step are written for readback. */
 LBM_API int lbm_step(lbm_ctx* ctx, int nsteps);
 
-/* Physics mode: nodes per thread of the step kernel, 0 = automatic (four for
- * fp16/bf16 storage when nx % 4 == 0 and the rows fill 128-wide warps, two
- * when nx is even and the rows fill 64-wide warps, else one), or 1, 2, 4.
- * All variants give bit-identical results; this is a tuning and testing
- * knob.  LBM_ERR_UNSUPPORTED for a variant the grid or precision cannot use. */
+/* Physics mode: kernel variant of the step.  0 = automatic (two nodes per
+ * thread when nx is even and the rows fill 64-wide warps, else one); 1, 2 or
+ * 4 nodes per thread (4: fp16/bf16 storage and nx % 4 == 0); 8 = one node per
+ * thread with the learned closure's hidden layer on the tensor cores (tcgen05;
+ * without a closure the same as 1).  The 1-, 2- and 4-node variants agree bit
+ * for bit except with a body force, where the one-node kernel's force terms
+ * differ in the last place in a few per cent of values.  A tuning and testing
+ * knob; LBM_ERR_UNSUPPORTED for a variant the grid or precision cannot use. */
 LBM_API int lbm_set_step_variant(lbm_ctx* ctx, int nodes_per_thread);
 
 /* Waits for the context's stream; returns LBM_ERR_NONFINITE if a NaN/Inf or

@@ -49,10 +49,11 @@ extern "C" {
 /* Installs a network on a physics-mode lattice whose descriptor has
  * smagorinsky_cs > 0 (the Cs0 that r scales); later steps use it.  net = NULL
  * removes it (plain Smagorinsky again).  The weights are copied.  By default
- * the step evaluates the 32 x 32 hidden layer on the tensor cores (tcgen05
- * MMA, bf16 activations and weights, fp32 accumulator in tensor memory, one
- * node per thread); lbm_set_step_variant(ctx, 1 or 2) selects the CUDA-core
- * evaluation (fp32 activations) instead. */
+ * the step evaluates the MLP on CUDA cores (fp32 activations, the weights as
+ * constant-bank operands, one or two nodes per thread);
+ * lbm_set_step_variant(ctx, 8) evaluates the 32 x 32 hidden layer on the
+ * tensor cores instead (tcgen05 MMA of the CTA's 128 nodes, bf16 activations
+ * and weights, fp32 accumulator in tensor memory). */
 LBM_API int lbm_set_closure(lbm_ctx* ctx, const float* net);
 
 /* Box filter of moment fields by `factor` along each axis (factor divides

@@ -321,14 +321,17 @@ def test_network_beats_constant_a_priori(gpu):
 
 @pytest.mark.parametrize("shape", [(32, 12, 10), (40, 9, 6)])
 def test_tensor_core_mlp_matches_cuda_core_mlp(gpu, oracle, shape):
-    """The default closure step evaluates the hidden layer with tcgen05 MMAs
-    (bf16 activations); the CUDA-core variant keeps fp32 activations.  Both
-    agree with the FP64 ExtStep closure at the physics-mode bar (3e-5 of the
-    velocity scale) and with each other; ny not a multiple of the CTA's four
-    rows exercises the rows that only take part in the MMA."""
+    """Variant 8 evaluates the hidden layer with tcgen05 MMAs (bf16
+    activations); the default CUDA-core path keeps fp32 activations.  Against
+    the FP64 ExtStep closure (fp32 activations in FP64) the CUDA-core path
+    meets the physics-mode bar, 3e-5 of the velocity scale after 40 steps; the
+    tensor-core path is held to 1e-4, since rounding the 32 activations to
+    bf16 (2^-9 relative) moves r, and with it tau_eff, by about that much.
+    ny not a multiple of the CTA's four rows exercises the rows that only take
+    part in the MMA."""
     net = _net(13)
     runs = []
-    for variant in (0, 1):
+    for variant in (8, 1):
         lat, st = _closure_pair(gpu, oracle, shape, net)
         lat.set_step_variant(variant)
         lat.step(40)
@@ -337,6 +340,7 @@ def test_tensor_core_mlp_matches_cuda_core_mlp(gpu, oracle, shape):
         lat.close()
     st.step(40)
     scale = np.abs(st.u).max()
-    for u in runs:
-        assert np.max(np.abs(u.T - st.u)) / scale <= 3e-5
-    assert np.max(np.abs(runs[0] - runs[1])) / scale <= 3e-5
+    assert np.max(np.abs(runs[1].T - st.u)) / scale <= 3e-5  # CUDA cores
+    assert np.max(np.abs(runs[0].T - st.u)) / scale <= 1e-4  # tensor cores
+    assert np.max(np.abs(runs[0] - runs[1])) / scale <= 1e-4
+    assert not np.array_equal(runs[0], runs[1])  # the two paths really differ
