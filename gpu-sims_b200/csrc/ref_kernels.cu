@@ -45,6 +45,25 @@ __device__ __forceinline__ float pull(const RefParams& p, const float* __restric
   return __ldg(fin + (size_t)I * p.n + src);
 }
 
+// The 19 pulls of a node.  Away from the y and z faces every source lies in
+// a row at a constant offset from the node's row, so only x is clamped (the
+// x faces fall inside ordinary warps, which then do not diverge); nodes on a
+// y or z face take the fully clamped path.
+__device__ __forceinline__ void pull_all(const RefParams& p, const float* __restrict__ fin, int x, int y,
+                                         int z, size_t nid, float (&g)[Q]) {
+  if (y > 0 && y < p.ny - 1 && z > 0 && z < p.nz - 1) {
+    const ptrdiff_t sy = p.nx, sz = (ptrdiff_t)p.nx * p.ny;
+    const float* row = fin + (nid - (size_t)x);  // (0, y, z)
+    static_for<0, Q>([&](auto I) {
+      constexpr int i = decltype(I)::value;
+      const int xs = cx(i) == 0 ? x : clamp_edge(x - cx(i), p.nx - 1);
+      g[i] = __ldg(row + (size_t)i * p.n + (-(cy(i) * sy + cz(i) * sz) + xs));
+    });
+  } else {
+    static_for<0, Q>([&](auto I) { g[I.value] = pull<decltype(I)::value>(p, fin, x, y, z); });
+  }
+}
+
 // compute_moments (shaders/compute_moments.comp.glsl:37-47): rho summed in
 // direction order, rho*u as signed sums, u = rho*u / rho guarded by 1e-12.
 // Also the outlet's upstream velocity (apply_boundaries.comp.glsl:112-119),
@@ -85,6 +104,10 @@ __global__ void __launch_bounds__(256)
   const size_t N = p.n;
   const size_t nid = (size_t)x + (size_t)p.nx * ((size_t)y + (size_t)p.ny * (size_t)z);
   const uint8_t fl = flags[nid];
+  // the pulls are issued before the flag is known (every source is in the
+  // grid), so a node costs one memory round trip, not two
+  float g[Q];
+  pull_all(p, fin, x, y, z, nid, g);
 
   if (fl & FLAG_SOLID) {
     // (1) solid: populations zeroed (apply_boundaries.comp.glsl:62-66); the
@@ -98,9 +121,6 @@ __global__ void __launch_bounds__(256)
     }
     return;
   }
-
-  float g[Q];
-  static_for<0, Q>([&](auto I) { g[I.value] = pull<decltype(I)::value>(p, fin, x, y, z); });
 
   // (2) post-stream bounce-back, sequential in i (apply_boundaries.comp.glsl:76-82):
   // if mask(x + c_i) (out of bounds = solid): f[opp i] := f[i].
