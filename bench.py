@@ -140,6 +140,24 @@ def dist_setup(n_gpus: int):
     return world, rank, local
 
 
+def max_over_ranks(v: float, world: int, device: str = "cuda") -> float:
+    """The slowest rank's time (every rank takes part; one all-reduce)."""
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_mlups(nodes_per_rank: int, steps: int, seconds_max: float, world: int) -> float:
+    """Whole-job rate: every rank advances its own replica of nodes_per_rank
+    nodes, so the job did world * nodes * steps updates in the slowest
+    rank's time."""
+    return world * nodes_per_rank * steps / seconds_max / 1e6
+
+
 def run_reference_arm(args, world, rank):
     """The CPU implementation of the same step (the oracle's float port of
     the stream-collide), on all host threads, on the same workload."""
@@ -220,12 +238,8 @@ def run_ours(args, world, rank, local):
             dist.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(v: float) -> float:
-        if world == 1:
-            return v
-        t = torch.tensor([v], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    def ranks_max(v: float) -> float:
+        return max_over_ranks(v, world, "cuda")
 
     mask, rho, u = make_inputs()
     n = mask.size
@@ -262,11 +276,11 @@ def run_ours(args, world, rank, local):
             lat.step(args.steps)
             e1.record(stream)
             torch.cuda.synchronize()
-        ms = max_over_ranks(e0.elapsed_time(e1))
+        ms = ranks_max(e0.elapsed_time(e1))
         lat.sync()
         lat.close()
         per_launch = ms / 1e3 / args.steps
-        return {"value": world * nodes * args.steps / (ms / 1e3) / 1e6, "unit": "MLUPS",
+        return {"value": aggregate_mlups(nodes, args.steps, ms / 1e3, world), "unit": "MLUPS",
                 "ms_per_step": ms / args.steps, "bytes_per_node": bpn,
                 "achieved_gbs": nodes * bpn / per_launch / 1e9,
                 "frac": nodes * bpn / per_launch / 1e9 / peak, "clocks": clk.summary()}
@@ -299,11 +313,11 @@ def run_ours(args, world, rank, local):
         rc = lib.lbm_read_moments(lat._h, r_out.ctypes.data, u_out.ctypes.data, lbm.U_F32X3)
         assert rc == 0
         torch.cuda.synchronize()
-        dt = max_over_ranks(time.perf_counter() - t0)
+        dt = ranks_max(time.perf_counter() - t0)
         lat.close()
         h2d = (m_h.nbytes + r_h.nbytes + u_h.nbytes) / args.steps
         d2h = 32 + (r_out.nbytes + u_out.nbytes) / args.steps
-        return {"value": world * n * args.steps / dt / 1e6, "unit": "MLUPS",
+        return {"value": aggregate_mlups(n, args.steps, dt, world), "unit": "MLUPS",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "what": "flags + initial moments uploaded from pinned host memory, per step one "
                         "lbm_step(1) and a read of the fp64 conservation sums, final rho/u read "

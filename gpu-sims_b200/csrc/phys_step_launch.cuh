@@ -10,6 +10,11 @@ namespace {
 #ifndef LBM_STEP2_MINB
 #define LBM_STEP2_MINB 5
 #endif
+// the 2-byte formats are issue-bound rather than memory-bound: their
+// residency bound is tuned separately
+#ifndef LBM_STEP2_MINB16
+#define LBM_STEP2_MINB16 5
+#endif
 // Residency bounds of the learned-closure kernels (the MLP's hidden layer
 // stays in registers: two nodes' worth in the pair kernel).
 #ifndef LBM_CLO_MINB
@@ -22,7 +27,8 @@ namespace {
 // Two nodes per thread (step_pairs(nx)): a warp covers 64 consecutive x.
 // SGS: 0 none, 1 Smagorinsky, 2 learned closure (net = the network).
 template <int PREC, int COLL, int SGS, bool FORCE, bool WRITE_MOMENTS, int P>
-__global__ void __launch_bounds__(STEP_THREADS, SGS == 2 ? LBM_CLO2_MINB : LBM_STEP2_MINB)
+__global__ void __launch_bounds__(STEP_THREADS, SGS == 2 ? LBM_CLO2_MINB
+                                                  : (PREC == LBM_PREC_F32 ? LBM_STEP2_MINB : LBM_STEP2_MINB16))
     k_phys_step2(PhysParams p, void* __restrict__ pop_v, const uint8_t* __restrict__ flags,
                  const uint32_t* __restrict__ links, float* __restrict__ rho_o,
                  float* __restrict__ u_o, unsigned* __restrict__ status,
