@@ -10,6 +10,7 @@
 
 #include "../../include/lbm.h"
 #include "d3q19.cuh"
+#include "lbm_internal.h"
 
 namespace {
 
@@ -89,27 +90,12 @@ int winding(const std::vector<P2>& poly, float px, float py) {
 
 }  // namespace
 
-extern "C" {
+namespace lbm {
 
-int lbm_lattice_tables(int32_t* c, float* w, int32_t* opp) {
-  for (int i = 0; i < 19; ++i) {
-    if (c) {
-      c[3 * i + 0] = lbm::cx(i);
-      c[3 * i + 1] = lbm::cy(i);
-      c[3 * i + 2] = lbm::cz(i);
-    }
-    if (w) w[i] = lbm::wf(i);
-    if (opp) opp[i] = lbm::opp(i);
-  }
-  return LBM_OK;
-}
-
-int lbm_voxelize_naca(const char* designation, int32_t nx, int32_t ny, int32_t nz, float chord_frac,
-                      float center_x_frac, float angle_of_attack_deg, uint8_t* mask, size_t n) {
+bool naca_perimeter(const char* designation, int32_t nx, int32_t ny, float chord_frac, float center_x_frac,
+                    float angle_of_attack_deg, std::vector<float>* xy) {
   Naca a;
-  if (!parse_naca(designation, &a)) return LBM_ERR_INVALID_ARG;
-  if (nx < 1 || ny < 1 || nz < 1 || !mask) return LBM_ERR_INVALID_ARG;
-  if (n != (size_t)nx * (size_t)ny * (size_t)nz) return LBM_ERR_INVALID_ARG;
+  if (!parse_naca(designation, &a) || nx < 1 || ny < 1) return false;
   // Preset geometry (src/main.cpp:1180-1190): chord in pixels, leading edge
   // half a chord upstream of the chord centre, on the domain's mid-height.
   const float chord = chord_frac * float(nx);
@@ -132,12 +118,43 @@ int lbm_voxelize_naca(const char* designation, int32_t nx, int32_t ny, int32_t n
   }
   for (int i = kSamples - 1; i >= 0; --i) poly.push_back(lower[i]);
   const float ca = std::cos(alpha), sa = std::sin(alpha);
-  for (P2& q : poly) {
-    const float xp = q.x * chord, yp = q.y * chord;
+  xy->resize(2 * poly.size());
+  for (size_t i = 0; i < poly.size(); ++i) {
+    const float xp = poly[i].x * chord, yp = poly[i].y * chord;
     const float xr = ca * xp - sa * yp;
     const float yr = sa * xp + ca * yp;
-    q = {xr + le_x, yr + le_y};
+    (*xy)[2 * i] = xr + le_x;
+    (*xy)[2 * i + 1] = yr + le_y;
   }
+  return true;
+}
+
+}  // namespace lbm
+
+extern "C" {
+
+int lbm_lattice_tables(int32_t* c, float* w, int32_t* opp) {
+  for (int i = 0; i < 19; ++i) {
+    if (c) {
+      c[3 * i + 0] = lbm::cx(i);
+      c[3 * i + 1] = lbm::cy(i);
+      c[3 * i + 2] = lbm::cz(i);
+    }
+    if (w) w[i] = lbm::wf(i);
+    if (opp) opp[i] = lbm::opp(i);
+  }
+  return LBM_OK;
+}
+
+int lbm_voxelize_naca(const char* designation, int32_t nx, int32_t ny, int32_t nz, float chord_frac,
+                      float center_x_frac, float angle_of_attack_deg, uint8_t* mask, size_t n) {
+  if (nx < 1 || ny < 1 || nz < 1 || !mask) return LBM_ERR_INVALID_ARG;
+  if (n != (size_t)nx * (size_t)ny * (size_t)nz) return LBM_ERR_INVALID_ARG;
+  std::vector<float> xy;
+  if (!lbm::naca_perimeter(designation, nx, ny, chord_frac, center_x_frac, angle_of_attack_deg, &xy))
+    return LBM_ERR_INVALID_ARG;
+  std::vector<P2> poly(xy.size() / 2);
+  for (size_t i = 0; i < poly.size(); ++i) poly[i] = {xy[2 * i], xy[2 * i + 1]};
   std::memset(mask, 0, n);
   for (int32_t y = 0; y < ny; ++y)
     for (int32_t x = 0; x < nx; ++x) {

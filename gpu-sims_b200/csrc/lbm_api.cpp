@@ -332,11 +332,8 @@ int lbm_set_closure(lbm_ctx* c, const float* net) {
   return LBM_OK;
 }
 
-int lbm_set_flags(lbm_ctx* c, const uint8_t* mask, size_t n) {
-  if (int rc = check_ctx(c)) return rc;
-  if (!mask) return fail(c, LBM_ERR_INVALID_ARG, "mask is NULL");
-  if (n != c->n) return fail(c, LBM_ERR_INVALID_ARG, "mask length must be Nx*Ny*Nz");
-  CK(cudaMemcpyAsync(c->mask, mask, n, cudaMemcpyHostToDevice, c->stream), "upload mask");
+// Classifies the mask already in c->mask (lbm_set_flags, lbm_set_flags_naca).
+static int classify_mask(lbm_ctx* c) {
   const int per[3] = {c->d.mode == LBM_MODE_PHYSICS ? c->d.periodic[0] : 0,
                       c->d.mode == LBM_MODE_PHYSICS ? c->d.periodic[1] : 0,
                       c->d.mode == LBM_MODE_PHYSICS ? c->d.periodic[2] : 0};
@@ -346,6 +343,26 @@ int lbm_set_flags(lbm_ctx* c, const uint8_t* mask, size_t n) {
   // new init; the reference step zeroes solids itself and can continue.
   if (c->d.mode == LBM_MODE_PHYSICS) c->initialized = false;
   return LBM_OK;
+}
+
+int lbm_set_flags(lbm_ctx* c, const uint8_t* mask, size_t n) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!mask) return fail(c, LBM_ERR_INVALID_ARG, "mask is NULL");
+  if (n != c->n) return fail(c, LBM_ERR_INVALID_ARG, "mask length must be Nx*Ny*Nz");
+  CK(cudaMemcpyAsync(c->mask, mask, n, cudaMemcpyHostToDevice, c->stream), "upload mask");
+  return classify_mask(c);
+}
+
+int lbm_set_flags_naca(lbm_ctx* c, const char* designation, float chord_frac, float center_x_frac,
+                       float angle_of_attack_deg) {
+  if (int rc = check_ctx(c)) return rc;
+  if (c->d.ny > 65535 * 8) return fail(c, LBM_ERR_UNSUPPORTED, "Ny above 524280");
+  bool bad = false;
+  const cudaError_t e = lbm::naca_mask_device(designation, c->d.nx, c->d.ny, c->d.nz, chord_frac,
+                                              center_x_frac, angle_of_attack_deg, c->mask, c->stream, &bad);
+  if (bad) return fail(c, LBM_ERR_INVALID_ARG, "designation must be four digits");
+  if (e != cudaSuccess) return cuda_fail(c, e, "voxelise");
+  return classify_mask(c);
 }
 
 int lbm_read_classification(lbm_ctx* c, uint32_t* out, size_t n) {

@@ -4,6 +4,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "../../include/lbm.h"
 #include "../../include/lbm_closure.h"
@@ -154,7 +155,16 @@ float round_bf16(float v);
 // Fills c.pp (padded geometry and physics parameters) from a physics-mode
 // descriptor; false if a slot array would exceed 2^32 elements.
 bool setup_physics(Ctx& c, const lbm_desc& d);
-int validate_desc(const lbm_desc* d);  // LBM_OK or an LBM_ERR_* (message set)
+int validate_desc(const lbm_desc* d);
+// NACA perimeter of lbm_voxelize_naca in lattice units (x0 y0 x1 y1 ...);
+// false for a designation that is not four digits (host_tools.cpp).
+bool naca_perimeter(const char* designation, int32_t nx, int32_t ny, float chord_frac, float center_x_frac,
+                    float angle_of_attack_deg, std::vector<float>* xy);
+// Device NACA mask into d_mask (voxel.cu); *bad_designation set instead of
+// launching when the designation is invalid.
+cudaError_t naca_mask_device(const char* designation, int32_t nx, int32_t ny, int32_t nz, float chord_frac,
+                             float center_x_frac, float angle_of_attack_deg, uint8_t* d_mask,
+                             cudaStream_t s, bool* bad_designation);  // LBM_OK or an LBM_ERR_* (message set)
 void set_thread_error(const char* msg);
 double bytes_per_node(const lbm_desc& d);
 

@@ -133,6 +133,7 @@ _SIGS = {
     "lbm_destroy": (C.c_int, [_P]),
     "lbm_set_stream": (C.c_int, [_P, _P]),
     "lbm_set_flags": (C.c_int, [_P, _P, C.c_size_t]),
+    "lbm_set_flags_naca": (C.c_int, [_P, C.c_char_p, C.c_float, C.c_float, C.c_float]),
     "lbm_read_classification": (C.c_int, [_P, _P, C.c_size_t]),
     "lbm_init_equilibrium": (C.c_int, [_P, C.c_float, C.POINTER(C.c_float)]),
     "lbm_init_from_moments": (C.c_int, [_P, _P, _P, C.c_int]),
@@ -149,6 +150,8 @@ _SIGS = {
     "lbm_lattice_tables": (C.c_int, [_P, _P, _P]),
     "lbm_voxelize_naca": (C.c_int, [C.c_char_p, C.c_int32, C.c_int32, C.c_int32, C.c_float,
                                     C.c_float, C.c_float, _P, C.c_size_t]),
+    "lbm_voxelize_naca_device": (C.c_int, [C.c_char_p, C.c_int32, C.c_int32, C.c_int32, C.c_float,
+                                           C.c_float, C.c_float, _P, C.c_size_t, _P]),
     "lbm_half_to_float": (C.c_int, [_P, _P, C.c_size_t]),
     "lbm_build_info": (C.c_char_p, []),
     "lbm_batch_schedule_default": (C.c_int, [C.POINTER(BatchSchedule)]),
@@ -252,6 +255,16 @@ def voxelize_naca(designation: str, nx: int, ny: int, nz: int, chord_frac: float
     return m
 
 
+def voxelize_naca_device(designation: str, nx: int, ny: int, nz: int, d_mask: int, n: int,
+                         chord_frac: float = 0.25, center_x_frac: float = 0.25,
+                         angle_of_attack_deg: float = 0.0, stream: int = 0) -> None:
+    """The mask of voxelize_naca written on the device into d_mask (a device
+    pointer to n = nx*ny*nz bytes) on `stream`; asynchronous."""
+    _check(load().lbm_voxelize_naca_device(designation.encode(), nx, ny, nz, chord_frac, center_x_frac,
+                                           angle_of_attack_deg, C.c_void_p(d_mask), n,
+                                           C.c_void_p(stream or None)))
+
+
 def half_to_float(h: np.ndarray) -> np.ndarray:
     h = np.ascontiguousarray(h, dtype=np.uint16)
     out = np.empty(h.shape, np.float32)
@@ -316,6 +329,12 @@ class Lattice:
     def set_flags(self, mask: np.ndarray) -> None:
         m = np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
         self._c(load().lbm_set_flags(self._h, _ptr(m), m.size))
+
+    def set_flags_naca(self, designation: str, chord_frac: float = 0.25, center_x_frac: float = 0.25,
+                       angle_of_attack_deg: float = 0.0) -> None:
+        """set_flags(voxelize_naca(...)) with the mask made on the device."""
+        self._c(load().lbm_set_flags_naca(self._h, designation.encode(), chord_frac, center_x_frac,
+                                          angle_of_attack_deg))
 
     def read_populations_shifted(self) -> np.ndarray:
         g = np.empty((19, self.n), np.float32)
@@ -549,14 +568,20 @@ def preset_desc(preset_idx: int, nx: int, ny: int, nz: int) -> Desc:
     return default_desc(nx=nx, ny=ny, nz=nz, tau=p.tau, u_inf=preset_u_inf(p))
 
 
-def apply_preset(lat: Lattice, preset_idx: int) -> np.ndarray:
+def apply_preset(lat: Lattice, preset_idx: int, device: bool = False) -> np.ndarray:
     """apply_preset (src/main.cpp:1167-1211): voxelise the airfoil, upload the
-    mask, run the equilibrium init.  Returns the mask."""
+    mask, run the equilibrium init.  Returns the mask.  device=True makes the
+    mask on the GPU (set_flags_naca; the same mask) and reads it back."""
     p = PRESETS[preset_idx]
     nx, ny, nz = lat.shape
-    mask = voxelize_naca(p.naca, nx, ny, nz, AIRFOIL_CHORD_LENGTH_FRAC, AIRFOIL_CHORD_CENTER_X_FRAC,
-                         p.angle_of_attack_deg)
-    lat.set_flags(mask)
+    if device:
+        lat.set_flags_naca(p.naca, AIRFOIL_CHORD_LENGTH_FRAC, AIRFOIL_CHORD_CENTER_X_FRAC,
+                           p.angle_of_attack_deg)
+        mask = lat.read_mask()
+    else:
+        mask = voxelize_naca(p.naca, nx, ny, nz, AIRFOIL_CHORD_LENGTH_FRAC, AIRFOIL_CHORD_CENTER_X_FRAC,
+                             p.angle_of_attack_deg)
+        lat.set_flags(mask)
     lat.init_equilibrium(1.0, tuple(lat.desc.u_inf))
     return mask
 

@@ -134,6 +134,15 @@ LBM_API int lbm_set_stream(lbm_ctx* ctx, void* stream);
  * Replaces obstacle_mask.upload (src/main.cpp:1190, :1366). */
 LBM_API int lbm_set_flags(lbm_ctx* ctx, const uint8_t* mask, size_t n);
 
+/* lbm_set_flags with the NACA preset mask made on the device
+ * (lbm_voxelize_naca_device into the context's mask, then classification):
+ * the same mask and classification as lbm_set_flags of the host mask of
+ * lbm_voxelize_naca with the context's Nx, Ny, Nz, without the host mask or
+ * its upload.  Replaces the voxelize_into + obstacle_mask.upload pair of
+ * apply_preset (src/main.cpp:1180-1190). */
+LBM_API int lbm_set_flags_naca(lbm_ctx* ctx, const char* designation, float chord_frac,
+                               float center_x_frac, float angle_of_attack_deg);
+
 /* Reads the per-node classification word: bit 0 = node is solid; bit i
  * (1..18) = mask at x + c_i is solid, out-of-bounds counting as solid on
  * non-periodic axes (shaders/apply_boundaries.comp.glsl:52-55,76-79). */
@@ -423,6 +432,17 @@ LBM_API int lbm_lattice_tables(int32_t* c, float* w, int32_t* opp);
 LBM_API int lbm_voxelize_naca(const char* designation, int32_t nx, int32_t ny,
                       int32_t nz, float chord_frac, float center_x_frac,
                       float angle_of_attack_deg, uint8_t* mask, size_t n);
+
+/* The same mask as lbm_voxelize_naca, produced on the device: the perimeter
+ * is built on the host as lbm_voxelize_naca builds it, and the winding test of
+ * every (x, y) column runs in a kernel on `stream` (a cudaStream_t; NULL = the
+ * legacy default stream), writing all n = Nx*Ny*Nz bytes of the device buffer
+ * d_mask.  Asynchronous; bit-identical to the host voxeliser.  Replaces
+ * naca::voxelize_into (src/main.cpp:254-312) where the mask goes to the GPU. */
+LBM_API int lbm_voxelize_naca_device(const char* designation, int32_t nx, int32_t ny,
+                      int32_t nz, float chord_frac, float center_x_frac,
+                      float angle_of_attack_deg, uint8_t* d_mask, size_t n,
+                      void* stream);
 
 /* binary16 -> binary32, as half_to_float (src/main.cpp:320-337). */
 LBM_API int lbm_half_to_float(const uint16_t* h, float* f, size_t n);
