@@ -293,6 +293,8 @@ int lbm_batch_create(const lbm_desc* descs, int n, lbm_batch** out) {
         d.body_accel[2] != 0.f)
       return bfail(nullptr, LBM_ERR_UNSUPPORTED,
                    "batched domains have no Smagorinsky term and no body force (use lbm_create)");
+    if (d.open_x[0] != LBM_OPEN_NONE || d.open_x[1] != LBM_OPEN_NONE)
+      return bfail(nullptr, LBM_ERR_UNSUPPORTED, "batched domains have no open faces (use lbm_create)");
   }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {

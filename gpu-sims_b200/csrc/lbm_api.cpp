@@ -75,6 +75,19 @@ int validate(const lbm_desc* d) {
     if (!(d->smagorinsky_cs >= 0.f) || !(d->trt_magic > 0.f))
       return fail(nullptr, LBM_ERR_INVALID_ARG, "smagorinsky_cs must be >= 0 and trt_magic > 0");
   }
+  for (int s = 0; s < 2; ++s) {
+    if (d->open_x[s] < LBM_OPEN_NONE || d->open_x[s] > LBM_OPEN_PRESSURE)
+      return fail(nullptr, LBM_ERR_INVALID_ARG, "open_x must be LBM_OPEN_NONE, _VELOCITY or _PRESSURE");
+    if (d->open_x[s] == LBM_OPEN_NONE) continue;
+    if (d->mode != LBM_MODE_PHYSICS || d->periodic[0])
+      return fail(nullptr, LBM_ERR_UNSUPPORTED, "open x faces need physics mode and a non-periodic x axis");
+    if (d->open_x[s] == LBM_OPEN_PRESSURE && !(d->open_rho[s] > 0.f && std::isfinite(d->open_rho[s])))
+      return fail(nullptr, LBM_ERR_INVALID_ARG, "open_rho of a pressure face must be finite and > 0");
+    const float* u = d->wall_velocity[s];
+    if (d->open_x[s] == LBM_OPEN_VELOCITY &&
+        !(std::fabs(u[0]) < 0.5f && std::isfinite(u[1]) && std::isfinite(u[2])))
+      return fail(nullptr, LBM_ERR_INVALID_ARG, "velocity of an open face must be finite with |u_x| < 0.5");
+  }
   return LBM_OK;
 }
 
@@ -158,6 +171,12 @@ bool setup_physics(Ctx& c, const lbm_desc& d) {
       p.wall[f][a] = d.wall_velocity[f][a];
       if (d.wall_velocity[f][a] != 0.f) p.any_moving_wall = 1;
     }
+  p.any_open = 0;
+  for (int s = 0; s < 2; ++s) {
+    p.open[s] = d.open_x[s];
+    p.open_rho[s] = d.open_rho[s];
+    if (d.open_x[s] != LBM_OPEN_NONE) p.any_open = 1;
+  }
   return true;
 }
 
@@ -297,6 +316,8 @@ int lbm_set_step_variant(lbm_ctx* c, int nodes_per_thread) {
   if (v == 2 && c->d.nx % 2) return fail(c, LBM_ERR_UNSUPPORTED, "two nodes per thread need an even nx");
   if (v == 4 && (c->d.nx % 4 || c->d.precision == LBM_PREC_F32))
     return fail(c, LBM_ERR_UNSUPPORTED, "four nodes per thread need nx % 4 == 0 and 2-byte storage");
+  if ((v == 4 || v == 8) && c->pp.any_open)
+    return fail(c, LBM_ERR_UNSUPPORTED, "open x faces run with one or two nodes per thread");
   CK(cudaStreamSynchronize(c->stream), "set_step_variant sync");
   for (auto& g : c->graph)
     if (g) {

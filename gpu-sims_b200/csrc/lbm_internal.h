@@ -70,6 +70,11 @@ struct PhysParams {
   float accel[3];
   float wall[6][3];
   int any_moving_wall;
+  // open x faces (enum lbm_open; [0] = x-, [1] = x+): a VELOCITY face takes
+  // its velocity from wall[0] / wall[1]
+  int open[2];
+  float open_rho[2];
+  int any_open;
 };
 
 struct Ctx;

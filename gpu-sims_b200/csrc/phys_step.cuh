@@ -84,6 +84,55 @@ __device__ __forceinline__ float wall_term(const PhysParams& p, int x, int y, in
   return 6.0f * wf(J) * cu;
 }
 
+// Open x face (Zou & He 1997; D3Q19 form of Hecht & Harting 2010): the five
+// populations entering through the face, c_x = SX (+1 at x = 0, -1 at
+// x = nx-1), rebuilt from the streamed ones before the collision:
+//   rho (1 - SX u_x) = S0 + 2 Sk      (S0: c_x = 0 sum, Sk: c_x = -SX sum)
+//   f_a = f_opp(a) + 6 w_a rho (c_a.u) - c_ay N_y - c_az N_z,
+//   N_t = (1/2) sum_{c_x = 0} f_i c_it - rho u_t / 3,
+// which returns exactly rho and rho u as the node's moments.  A VELOCITY face
+// knows u and solves for rho, a PRESSURE face knows rho (u_y = u_z = 0) and
+// solves for u_x.  On shifted storage v = SC (f - w) the weights cancel:
+// S0 + 2 Sk = 1 + (V0 + 2 Vk) / SC and the c_t-weighted sums of w vanish.
+// at(i) is the node's value of direction i.
+template <int SX, class At>
+__device__ __forceinline__ void zou_he(const PhysParams& p, float sc, float inv_sc, At&& at) {
+  constexpr int side = SX > 0 ? 0 : 1;
+  float v0 = 0.0f, vk = 0.0f, my = 0.0f, mz = 0.0f;
+  static_for<0, Q>([&](auto I) {
+    constexpr int i = decltype(I)::value;
+    if constexpr (cx(i) == 0) {
+      v0 += at(i);
+      if constexpr (cy(i) != 0) my += float(cy(i)) * at(i);
+      if constexpr (cz(i) != 0) mz += float(cz(i)) * at(i);
+    } else if constexpr (cx(i) == -SX) {
+      vk += at(i);
+    }
+  });
+  const float m = 1.0f + (v0 + 2.0f * vk) * inv_sc;
+  float rho, ux, uy, uz;
+  if (p.open[side] == LBM_OPEN_VELOCITY) {
+    ux = p.wall[side][0];
+    uy = p.wall[side][1];
+    uz = p.wall[side][2];
+    rho = m / (1.0f - float(SX) * ux);
+  } else {
+    rho = p.open_rho[side];
+    ux = float(SX) * (1.0f - m / rho);
+    uy = 0.0f;
+    uz = 0.0f;
+  }
+  const float ny = 0.5f * my - sc * rho * uy * (1.0f / 3.0f);
+  const float nz = 0.5f * mz - sc * rho * uz * (1.0f / 3.0f);
+  static_for<0, Q>([&](auto I) {
+    constexpr int i = decltype(I)::value;
+    if constexpr (cx(i) == SX) {
+      const float cu = float(SX) * ux + float(cy(i)) * uy + float(cz(i)) * uz;
+      at(i) = at(opp(i)) + sc * (6.0f * wf(i)) * rho * cu - float(cy(i)) * ny - float(cz(i)) * nz;
+    }
+  });
+}
+
 // Collision on shifted populations in storage units v = SC (f - w), in
 // place, written per opposite pair (a, b): with cu = c_a . u the equilibrium
 // splits into an even part  w (drho + rho (4.5 cu^2 - 1.5 u.u))  shared by a
@@ -405,6 +454,11 @@ __device__ __forceinline__ void step_row(const PhysParams& p, const CloNet<SGS>&
     });
   }
 
+  if (p.any_open && fluid) {
+    if (xlo && p.open[0] != LBM_OPEN_NONE) zou_he<1>(p, S::SC, S::INV, [&](int i) -> float& { return g[i]; });
+    if (xhi && p.open[1] != LBM_OPEN_NONE) zou_he<-1>(p, S::SC, S::INV, [&](int i) -> float& { return g[i]; });
+  }
+
   float rho, ux, uy, uz;
   collide<COLL, SGS, FORCE, PREC>(p, net, g, rho, ux, uy, uz);
 
@@ -605,6 +659,12 @@ __device__ __forceinline__ void step_row2(const PhysParams& p, const CloNet<SGS>
   };
   if (fluidA && (flA & FLAG_SOLID_LINK)) solid_fix(IC<0>{}, nid, lnA, w, xloA, false);
   if (fluidB && (flB & FLAG_SOLID_LINK)) solid_fix(IC<1>{}, nid + 1, lnB, wB, false, xhiB);
+  if (p.any_open) {
+    if (fluidA && xloA && p.open[0] != LBM_OPEN_NONE)
+      zou_he<1>(p, S::SC, S::INV, [&](int i) -> float& { return g2[i].x; });
+    if (fluidB && xhiB && p.open[1] != LBM_OPEN_NONE)
+      zou_he<-1>(p, S::SC, S::INV, [&](int i) -> float& { return g2[i].y; });
+  }
 
   float2 r2, ux2, uy2, uz2;
   collide_t<Ops2, COLL, SGS, FORCE, PREC>(p, net, g2, r2, ux2, uy2, uz2);

@@ -142,7 +142,7 @@ template <> CloNet<2> net_of<2>(const Ctx& c) {
 // step_pairs(nx), else one.
 inline bool use_quads(const Ctx& c) {
   const int nx = c.pp.g.nx;
-  if (c.d.precision == LBM_PREC_F32 || c.closure || nx % 4) return false;
+  if (c.d.precision == LBM_PREC_F32 || c.closure || c.pp.any_open || nx % 4) return false;
   return c.step_variant == 4 || (c.step_variant == 0 && step_quads(nx));
 }
 inline bool use_pairs(const Ctx& c) {

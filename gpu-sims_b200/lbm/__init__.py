@@ -37,6 +37,7 @@ COLL_BGK, COLL_TRT = 0, 1
 UROUND_NONE, UROUND_RTE, UROUND_RTZ = 0, 1, 2
 U_F32X3, U_F16X4, U_F32X4 = 0, 1, 2
 FACE_XM, FACE_XP, FACE_YM, FACE_YP, FACE_ZM, FACE_ZP = range(6)
+OPEN_NONE, OPEN_VELOCITY, OPEN_PRESSURE = 0, 1, 2
 
 ERR_NAMES = {OK: "OK", ERR_INVALID_ARG: "INVALID_ARG", ERR_CUDA: "CUDA", ERR_NO_DEVICE: "NO_DEVICE",
              ERR_OUT_OF_MEMORY: "OUT_OF_MEMORY", ERR_STATE: "STATE", ERR_UNSUPPORTED: "UNSUPPORTED",
@@ -60,6 +61,7 @@ class Desc(C.Structure):
         ("wall_velocity", (C.c_float * 3) * 6),
         ("u_inf", C.c_float * 3), ("rho0", C.c_float),
         ("ref_inlet_outlet", C.c_int32), ("ref_free_slip", C.c_int32), ("ref_u_round", C.c_int32),
+        ("open_x", C.c_int32 * 2), ("open_rho", C.c_float * 2),
     ]
 
 
@@ -276,7 +278,7 @@ def default_desc(**kw) -> Desc:
     d = Desc()
     _check(load().lbm_desc_default(C.byref(d)))
     for k, v in kw.items():
-        if k in ("periodic", "body_accel", "u_inf"):
+        if k in ("periodic", "body_accel", "u_inf", "open_x", "open_rho"):
             arr = getattr(d, k)
             for i, x in enumerate(v):
                 arr[i] = x

@@ -74,6 +74,15 @@ enum lbm_u_round   { LBM_UROUND_NONE = 0, LBM_UROUND_RTE = 1, LBM_UROUND_RTZ = 2
 enum lbm_u_format  { LBM_U_F32X3 = 0,   /* float[N][3]                        */
                      LBM_U_F16X4 = 1,   /* uint16 half[N][4], w=0: rgba16f    */
                      LBM_U_F32X4 = 2 }; /* float[N][4], w=0                   */
+/* Open x faces (physics mode, x not periodic): the populations entering
+ * through the face are rebuilt by the non-equilibrium bounce-back of Zou & He
+ * (1997) in its D3Q19 form (Hecht & Harting 2010) instead of being bounced
+ * back.  VELOCITY prescribes u = wall_velocity[face]; PRESSURE prescribes
+ * rho = open_rho[x side] with zero tangential velocity.  The reference's
+ * -X inlet / +X outlet (shaders/apply_boundaries.comp.glsl:86-130) write
+ * equilibria; these are the Zou-He faces its notes plan as the upgrade
+ * (docs/notes.md:5-7, 23-24). */
+enum lbm_open      { LBM_OPEN_NONE = 0, LBM_OPEN_VELOCITY = 1, LBM_OPEN_PRESSURE = 2 };
 /* Faces, for per-face wall velocities: x-, x+, y-, y+, z-, z+. */
 enum lbm_face { LBM_FACE_XM = 0, LBM_FACE_XP, LBM_FACE_YM, LBM_FACE_YP,
                 LBM_FACE_ZM, LBM_FACE_ZP };
@@ -98,6 +107,9 @@ typedef struct lbm_desc {
     int32_t  ref_inlet_outlet;  /* regime 3 of apply_boundaries: 1 = on       */
     int32_t  ref_free_slip;     /* regime 4 of apply_boundaries: 1 = on       */
     int32_t  ref_u_round;       /* enum lbm_u_round, default RTE              */
+    /* physics mode: open x faces, [0] = x-, [1] = x+ (enum lbm_open) */
+    int32_t  open_x[2];
+    float    open_rho[2];       /* density of a PRESSURE face                */
 } lbm_desc;
 
 typedef struct lbm_info {

@@ -76,23 +76,28 @@ struct ExtP {
   double smag_cs;
   double accel[3];
   double wall[6][3];
+  int open[2];    // open x faces: 0 none, 1 velocity (u = wall[side]), 2 pressure
+  double open_rho[2];
   int has_net;    // learned closure: Cs^2 = smag_cs^2 * r(Pi, rho)
   double net[NET_FLOATS];
 };
 
-// ip: nx ny nz px py pz collision;
-// dp: tau trt_magic smag_cs accel[3] wall[18] has_net [net[NET_FLOATS] if has_net]
+// ip: nx ny nz px py pz collision open[2];
+// dp: tau trt_magic smag_cs accel[3] wall[18] open_rho[2] has_net
+//     [net[NET_FLOATS] if has_net]
 inline ExtP make_ext(const int* ip, const double* dp) {
   ExtP p;
   p.nx = ip[0]; p.ny = ip[1]; p.nz = ip[2];
   p.periodic[0] = ip[3]; p.periodic[1] = ip[4]; p.periodic[2] = ip[5];
   p.collision = ip[6];
+  p.open[0] = ip[7]; p.open[1] = ip[8];
   p.tau = dp[0]; p.trt_magic = dp[1]; p.smag_cs = dp[2];
   for (int a = 0; a < 3; ++a) p.accel[a] = dp[3 + a];
   for (int f = 0; f < 6; ++f)
     for (int a = 0; a < 3; ++a) p.wall[f][a] = dp[6 + 3 * f + a];
-  p.has_net = dp[24] != 0.0;
-  for (int k = 0; k < NET_FLOATS; ++k) p.net[k] = p.has_net ? dp[25 + k] : 0.0;
+  p.open_rho[0] = dp[24]; p.open_rho[1] = dp[25];
+  p.has_net = dp[26] != 0.0;
+  for (int k = 0; k < NET_FLOATS; ++k) p.net[k] = p.has_net ? dp[27 + k] : 0.0;
   return p;
 }
 
@@ -151,6 +156,49 @@ OX_HD inline T incoming(const ExtP& p, const uint8_t* mask, const T* f, int x, i
     v += T(6.0 * weight<double>(i) * cu);
   }
   return v;
+}
+
+// Open x face: the populations entering through it (c_x = +1 at x = 0,
+// -1 at x = nx-1) rebuilt from the streamed ones by the non-equilibrium
+// bounce-back of Zou & He (1997), D3Q19 form (Hecht & Harting 2010):
+//   rho (1 - s u_x) = sum_{c_x=0} f + 2 sum_{c_x=-s} f,
+//   f_i = f_opp(i) + 6 w_i rho (c_i.u) - c_iy N_y - c_iz N_z,
+//   N_t = 1/2 sum_{c_x=0} f c_t - rho u_t / 3.
+// Velocity faces know u (wall[side]) and solve for rho; pressure faces know
+// rho with u_y = u_z = 0 and solve for u_x.  Written from the definitions,
+// independently of the kernels' shifted-storage form.
+template <class T>
+OX_HD inline void open_face(const ExtP& p, T* v, int x) {
+  int side;
+  if (x == 0 && p.open[0]) side = 0;
+  else if (x == p.nx - 1 && p.open[1]) side = 1;
+  else return;
+  const int s = side == 0 ? 1 : -1;
+  T s0 = 0, sk = 0, my = 0, mz = 0;
+  for (int i = 0; i < 19; ++i) {
+    if (cc(i, 0) == 0) {
+      s0 += v[i];
+      my += T(cc(i, 1)) * v[i];
+      mz += T(cc(i, 2)) * v[i];
+    } else if (cc(i, 0) == -s) {
+      sk += v[i];
+    }
+  }
+  T rho, u[3];
+  if (p.open[side] == 1) {
+    for (int a = 0; a < 3; ++a) u[a] = T(p.wall[side][a]);
+    rho = (s0 + T(2) * sk) / (T(1) - T(s) * u[0]);
+  } else {
+    rho = T(p.open_rho[side]);
+    u[0] = T(s) * (T(1) - (s0 + T(2) * sk) / rho);
+    u[1] = u[2] = T(0);
+  }
+  const T Ny = my / T(2) - rho * u[1] / T(3), Nz = mz / T(2) - rho * u[2] / T(3);
+  for (int i = 0; i < 19; ++i) {
+    if (cc(i, 0) != s) continue;
+    const T cu = T(cc(i, 0)) * u[0] + T(cc(i, 1)) * u[1] + T(cc(i, 2)) * u[2];
+    v[i] = v[opp(i)] + T(6) * weight<T>(i) * rho * cu - T(cc(i, 1)) * Ny - T(cc(i, 2)) * Nz;
+  }
 }
 
 // Moments (u with the Guo half-force shift) and the collision, in place.

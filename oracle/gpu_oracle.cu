@@ -31,6 +31,7 @@ __global__ void k_step(ox::ExtP p, const uint8_t* mask, const double* fin, doubl
   }
   double v[19];
   for (int i = 0; i < 19; ++i) v[i] = ox::incoming<double>(p, mask, fin, x, y, z, i, N);
+  ox::open_face<double>(p, v, x);
   double r, ux, uy, uz;
   ox::ext_collide_node<double>(p, v, r, ux, uy, uz);
   for (int i = 0; i < 19; ++i) fout[i * N + n] = v[i];

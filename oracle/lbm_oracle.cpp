@@ -263,6 +263,7 @@ static void ext_step_t(const int* ip, const double* dp, const uint8_t* mask, T* 
           }
           T v[19];
           for (int i = 0; i < 19; ++i) v[i] = ox::incoming<T>(p, mask, f, x, y, z, i, N);
+          ox::open_face<T>(p, v, x);
           T r, ux, uy, uz;
           ox::ext_collide_node<T>(p, v, r, ux, uy, uz);
           for (int i = 0; i < 19; ++i) g[i * N + n] = v[i];

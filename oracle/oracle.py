@@ -143,11 +143,12 @@ class RefState:
         return out
 
 
-def _ext_dp(tau, trt_magic, smag_cs, accel, wall, net):
+def _ext_dp(tau, trt_magic, smag_cs, accel, wall, net, open_rho=(0.0, 0.0)):
     """Double parameters of ExtStep (ext_step.h make_ext): tau, Lambda, Cs,
-    accel[3], wall[6][3], has_net, then the network (its weights as the
-    kernels use them, rounded to bf16) if one is given."""
-    parts = [[tau, trt_magic, smag_cs], np.asarray(accel, np.float64), np.asarray(wall, np.float64).reshape(-1)]
+    accel[3], wall[6][3], open_rho[2], has_net, then the network (its weights
+    as the kernels use them, rounded to bf16) if one is given."""
+    parts = [[tau, trt_magic, smag_cs], np.asarray(accel, np.float64), np.asarray(wall, np.float64).reshape(-1),
+             np.asarray(open_rho, np.float64)]
     if net is None:
         parts.append([0.0])
     else:
@@ -161,14 +162,14 @@ class ExtState:
 
     def __init__(self, shape, periodic=(0, 0, 0), tau=0.6, collision=0, trt_magic=3.0 / 16.0,
                  smag_cs=0.0, accel=(0.0, 0.0, 0.0), wall=None, mask=None, dtype=np.float64,
-                 net=None):
+                 net=None, open_x=(0, 0), open_rho=(0.0, 0.0)):
         self.shape = tuple(shape)
         nx, ny, nz = self.shape
         self.n = nx * ny * nz
         self.dtype = np.dtype(dtype)
-        self.ip = np.array([nx, ny, nz, *periodic, collision], np.int32)
+        self.ip = np.array([nx, ny, nz, *periodic, collision, *open_x], np.int32)
         w = np.zeros((6, 3)) if wall is None else np.asarray(wall, np.float64).reshape(6, 3)
-        self.dp = _ext_dp(tau, trt_magic, smag_cs, accel, w, net)
+        self.dp = _ext_dp(tau, trt_magic, smag_cs, accel, w, net, open_rho)
         self.mask = np.zeros(self.n, np.uint8) if mask is None else np.ascontiguousarray(mask, np.uint8).reshape(-1)
         self.f = np.zeros((19, self.n), self.dtype)
         self.rho = np.zeros(self.n, self.dtype)
@@ -210,15 +211,16 @@ class ExtStateGPU:
     bit for bit); device memory through torch.  For full-size FP64 runs."""
 
     def __init__(self, shape, periodic=(0, 0, 0), tau=0.6, collision=0, trt_magic=3.0 / 16.0,
-                 smag_cs=0.0, accel=(0.0, 0.0, 0.0), wall=None, mask=None, net=None):
+                 smag_cs=0.0, accel=(0.0, 0.0, 0.0), wall=None, mask=None, net=None, open_x=(0, 0),
+                 open_rho=(0.0, 0.0)):
         import torch
         self.torch = torch
         self.shape = tuple(shape)
         nx, ny, nz = self.shape
         self.n = nx * ny * nz
-        self.ip = np.array([nx, ny, nz, *periodic, collision], np.int32)
+        self.ip = np.array([nx, ny, nz, *periodic, collision, *open_x], np.int32)
         w = np.zeros((6, 3)) if wall is None else np.asarray(wall, np.float64).reshape(6, 3)
-        self.dp = _ext_dp(tau, trt_magic, smag_cs, accel, w, net)
+        self.dp = _ext_dp(tau, trt_magic, smag_cs, accel, w, net, open_rho)
         m = np.zeros(self.n, np.uint8) if mask is None else np.ascontiguousarray(mask, np.uint8).reshape(-1)
         dev = torch.device("cuda")
         self.mask = torch.from_numpy(m).to(dev)
