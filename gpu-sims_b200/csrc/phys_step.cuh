@@ -109,16 +109,18 @@ __device__ __forceinline__ void zou_he(const PhysParams& p, float sc, float inv_
       vk += at(i);
     }
   });
-  const float m = 1.0f + (v0 + 2.0f * vk) * inv_sc;
+  const float dm = (v0 + 2.0f * vk) * inv_sc;  // S0 + 2 Sk - 1
   float rho, ux, uy, uz;
   if (p.open[side] == LBM_OPEN_VELOCITY) {
     ux = p.wall[side][0];
     uy = p.wall[side][1];
     uz = p.wall[side][2];
-    rho = m / (1.0f - float(SX) * ux);
+    rho = (1.0f + dm) / (1.0f - float(SX) * ux);
   } else {
+    // u_x = SX (1 - (1 + dm) / rho) in deviation form: rho - 1 is exact for
+    // rho in [0.5, 2], so a small u_x does not come from cancelling ~1 terms
     rho = p.open_rho[side];
-    ux = float(SX) * (1.0f - m / rho);
+    ux = float(SX) * (((rho - 1.0f) - dm) / rho);
     uy = 0.0f;
     uz = 0.0f;
   }
