@@ -49,6 +49,10 @@ __host__ __device__ constexpr int pair_b(int p) { return opp(pair_a(p)); }
 constexpr uint8_t FLAG_SOLID = 1u;     // mask value 1
 constexpr uint8_t FLAG_BOUNDARY = 2u;  // fluid node with a blocked link
 constexpr uint8_t FLAG_SOLID_LINK = 4u;  // ... of which one ends at a solid node of the grid
+// Fluid node on an open x face (physics mode): the row kernels leave it to
+// the face kernel, as they leave solid nodes alone.
+constexpr uint8_t FLAG_OPEN = 8u;
+constexpr uint8_t FLAG_SKIP = FLAG_SOLID | FLAG_OPEN;
 
 // ---------------------------------------------------------------------------
 // Reference-literal arithmetic.  Each operation is a separately rounded fp32

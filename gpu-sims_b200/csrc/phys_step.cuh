@@ -359,24 +359,30 @@ __device__ __forceinline__ uint32_t offs(const PhysGeom& G, const Wrap& w) {
 // One warp updates nodes x0 .. x0+31 of row (y, z); y < ny (the caller's
 // test is uniform over the warp).  Used by the single-domain kernel and by
 // the batched kernels (phys_batch.cu).
-template <int PREC, int COLL, int SGS, bool FORCE, bool WRITE_MOMENTS, int P>
+//
+// FACE: the open-face variant.  Each lane updates its own node (x0, y, z)
+// with every neighbour slot accessed directly (no shuffles), lane_ok false
+// for idle lanes, and the Zou-He reconstruction before the collision.  The
+// row kernels skip these nodes (FLAG_OPEN); the two sets of nodes read and
+// write disjoint slots, so the face kernel may run after them.
+template <int PREC, int COLL, int SGS, bool FORCE, bool WRITE_MOMENTS, int P, bool FACE = false>
 __device__ __forceinline__ void step_row(const PhysParams& p, const CloNet<SGS>& net,
                                          void* __restrict__ pop_v,
                                          const uint8_t* __restrict__ flags,
                                          const uint32_t* __restrict__ links,
                                          float* __restrict__ rho_o, float* __restrict__ u_o,
                                          unsigned* __restrict__ status, const int x0, const int y,
-                                         const int z) {
+                                         const int z, const bool lane_ok = true) {
   using S = Store<PREC>;
   using T = typename S::T;
   const PhysGeom& G = p.g;
   const int lane = threadIdx.x & 31;
-  const int x = x0 + lane;
+  const int x = FACE ? x0 : x0 + lane;
   bool row_ok = true;  // y < ny; only the tensor-core closure runs rows beyond
   if constexpr (SGS == 3) row_ok = net.row_ok;
-  const bool valid = x < G.nx && row_ok;
+  const bool valid = FACE ? lane_ok : x < G.nx && row_ok;
   const int xc = x < G.nx ? x : G.nx - 1;  // in-bounds address for idle lanes
-  const bool edge = (lane == 31) || (x >= G.nx - 1);  // touches x+1 itself
+  const bool edge = FACE || (lane == 31) || (x >= G.nx - 1);  // touches x+1 itself
   const uint32_t N = (uint32_t)G.n;
   const uint32_t nid = (uint32_t)xc + (uint32_t)G.nx * ((uint32_t)y + (uint32_t)G.ny * (uint32_t)z);
   T* pop = reinterpret_cast<T*>(pop_v);
@@ -435,7 +441,7 @@ __device__ __forceinline__ void step_row(const PhysParams& p, const CloNet<SGS>&
     });
   }
 
-  const bool fluid = valid && !(fl & FLAG_SOLID);
+  const bool fluid = valid && !(fl & (FACE ? FLAG_SOLID : FLAG_SKIP));
   // Links into interior solid nodes (resting walls) need the classification
   // word: a second, rare round trip.
   if (fluid && (fl & FLAG_SOLID_LINK)) {
@@ -456,9 +462,11 @@ __device__ __forceinline__ void step_row(const PhysParams& p, const CloNet<SGS>&
     });
   }
 
-  if (p.any_open && fluid) {
-    if (xlo && p.open[0] != LBM_OPEN_NONE) zou_he<1>(p, S::SC, S::INV, [&](int i) -> float& { return g[i]; });
-    if (xhi && p.open[1] != LBM_OPEN_NONE) zou_he<-1>(p, S::SC, S::INV, [&](int i) -> float& { return g[i]; });
+  if constexpr (FACE) {
+    if (fluid && xlo && p.open[0] != LBM_OPEN_NONE)
+      zou_he<1>(p, S::SC, S::INV, [&](int i) -> float& { return g[i]; });
+    if (fluid && xhi && p.open[1] != LBM_OPEN_NONE)
+      zou_he<-1>(p, S::SC, S::INV, [&](int i) -> float& { return g[i]; });
   }
 
   float rho, ux, uy, uz;
@@ -638,8 +646,8 @@ __device__ __forceinline__ void step_row2(const PhysParams& p, const CloNet<SGS>
       if (yz_fwd || (DX > 0 && xhiB)) g2[b].y = fmaf(S::SC, wall_term<b>(p, xc + 1, y, z), g2[b].y);
     });
   }
-  const bool fluidA = valid && !(flA & FLAG_SOLID);
-  const bool fluidB = valid && !(flB & FLAG_SOLID);
+  const bool fluidA = valid && !(flA & FLAG_SKIP);
+  const bool fluidB = valid && !(flB & FLAG_SKIP);
   auto solid_fix = [&](auto lane_sel, uint32_t nidn, uint32_t ln, const Wrap& wn, bool xlo, bool xhi) {
     constexpr bool B = decltype(lane_sel)::value != 0;
     auto at = [&](int i) -> float& { return B ? g2[i].y : g2[i].x; };
@@ -661,12 +669,6 @@ __device__ __forceinline__ void step_row2(const PhysParams& p, const CloNet<SGS>
   };
   if (fluidA && (flA & FLAG_SOLID_LINK)) solid_fix(IC<0>{}, nid, lnA, w, xloA, false);
   if (fluidB && (flB & FLAG_SOLID_LINK)) solid_fix(IC<1>{}, nid + 1, lnB, wB, false, xhiB);
-  if (p.any_open) {
-    if (fluidA && xloA && p.open[0] != LBM_OPEN_NONE)
-      zou_he<1>(p, S::SC, S::INV, [&](int i) -> float& { return g2[i].x; });
-    if (fluidB && xhiB && p.open[1] != LBM_OPEN_NONE)
-      zou_he<-1>(p, S::SC, S::INV, [&](int i) -> float& { return g2[i].y; });
-  }
 
   float2 r2, ux2, uy2, uz2;
   collide_t<Ops2, COLL, SGS, FORCE, PREC>(p, net, g2, r2, ux2, uy2, uz2);
@@ -852,7 +854,7 @@ __device__ __forceinline__ void step_row4(const PhysParams& p, const CloNet<SGS>
                          (uint8_t)(fl4 >> 24)};
   bool fluid[4];
 #pragma unroll
-  for (int k = 0; k < 4; ++k) fluid[k] = valid && !(fl[k] & FLAG_SOLID);
+  for (int k = 0; k < 4; ++k) fluid[k] = valid && !(fl[k] & FLAG_SKIP);
   // links into interior solids, per node (rare)
   auto solid_fix = [&](auto kk, const Wrap& wn, bool xlo, bool xhi) {
     constexpr int k = decltype(kk)::value;

@@ -51,6 +51,25 @@ __global__ void __launch_bounds__(STEP_THREADS, SGS == 2 ? LBM_CLO_MINB : LBM_ST
                                                      status, blockIdx.x * 32, y, blockIdx.z);
 }
 
+// Open x faces: one thread per face node, lanes over (y, z), blockIdx.y
+// the side (0: x = 0, 1: x = nx-1).  Runs after the row kernel of the same
+// step, which leaves these nodes alone (FLAG_OPEN).
+template <int PREC, int COLL, int SGS, bool FORCE, bool WRITE_MOMENTS, int P>
+__global__ void __launch_bounds__(128)
+    k_phys_face(PhysParams p, void* __restrict__ pop_v, const uint8_t* __restrict__ flags,
+                const uint32_t* __restrict__ links, float* __restrict__ rho_o,
+                float* __restrict__ u_o, unsigned* __restrict__ status,
+                const __grid_constant__ CloNet<SGS> net) {
+  const int side = blockIdx.y;
+  if (p.open[side] == LBM_OPEN_NONE) return;  // uniform over the block
+  const int nyz = p.g.ny * p.g.nz;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int tc = t < nyz ? t : nyz - 1;  // idle lanes take part in the shuffles
+  step_row<PREC, COLL, SGS, FORCE, WRITE_MOMENTS, P, true>(p, net, pop_v, flags, links, rho_o, u_o,
+                                                          status, side ? p.g.nx - 1 : 0, tc % p.g.ny,
+                                                          tc / p.g.ny, t < nyz);
+}
+
 #ifndef LBM_STEP4_MINB
 #define LBM_STEP4_MINB 3
 #endif
@@ -152,7 +171,7 @@ inline bool use_pairs(const Ctx& c) {
 }
 
 template <int PREC, int COLL, int SGS, bool FORCE>
-cudaError_t launch_step(const Ctx& c, int P, bool wm, cudaStream_t s) {
+cudaError_t launch_rows(const Ctx& c, int P, bool wm, cudaStream_t s) {
   const PhysGeom& G = c.pp.g;
   const CloNet<SGS> net = net_of<SGS>(c);
   const dim3 blk(32, STEP_BY, 1);
@@ -194,6 +213,25 @@ cudaError_t launch_step(const Ctx& c, int P, bool wm, cudaStream_t s) {
     if (P) LBM_STEP_LAUNCH(false, 1); else LBM_STEP_LAUNCH(false, 0);
   }
 #undef LBM_STEP_LAUNCH
+  return cudaGetLastError();
+}
+
+// One step: the row kernel, then (open x faces only) the face kernel.
+template <int PREC, int COLL, int SGS, bool FORCE>
+cudaError_t launch_step(const Ctx& c, int P, bool wm, cudaStream_t s) {
+  const cudaError_t e = launch_rows<PREC, COLL, SGS, FORCE>(c, P, wm, s);
+  if (e != cudaSuccess || !c.pp.any_open) return e;
+  const CloNet<SGS> net = net_of<SGS>(c);
+  const dim3 grd((c.pp.g.ny * c.pp.g.nz + 127) / 128, 2, 1);
+#define LBM_FACE_LAUNCH(WM, PAR)                                          \
+  k_phys_face<PREC, COLL, SGS, FORCE, WM, PAR><<<grd, 128, 0, s>>>(       \
+      c.pp, c.pop, c.flags, c.links, c.rho, c.u, c.status, net)
+  if (wm) {
+    if (P) LBM_FACE_LAUNCH(true, 1); else LBM_FACE_LAUNCH(true, 0);
+  } else {
+    if (P) LBM_FACE_LAUNCH(false, 1); else LBM_FACE_LAUNCH(false, 0);
+  }
+#undef LBM_FACE_LAUNCH
   return cudaGetLastError();
 }
 

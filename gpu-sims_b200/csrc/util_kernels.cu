@@ -11,12 +11,13 @@ namespace {
 // x + c_i is solid, where a neighbour outside the box counts as solid on a
 // non-periodic axis (mask_at, shaders/apply_boundaries.comp.glsl:52-55) and
 // wraps on a periodic one.  FLAG_BOUNDARY marks fluid nodes with any link
-// bit (the reference-mode step reads the word there); FLAG_SOLID_LINK those
+// bit (the reference-mode step reads the word there); FLAG_OPEN fluid nodes on
+// an open x face; FLAG_SOLID_LINK those
 // with a link to a solid node of the grid (the physics-mode step derives
 // wall links from the coordinates and reads the word only there).
 __global__ void __launch_bounds__(256)
-    k_classify(int nx, int ny, int nz, int px, int py, int pz, const uint8_t* __restrict__ mask,
-               uint8_t* __restrict__ flags, uint32_t* __restrict__ links) {
+    k_classify(int nx, int ny, int nz, int px, int py, int pz, int open_lo, int open_hi,
+               const uint8_t* __restrict__ mask, uint8_t* __restrict__ flags, uint32_t* __restrict__ links) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z * blockDim.z + threadIdx.z;
@@ -40,8 +41,10 @@ __global__ void __launch_bounds__(256)
     if (s) L |= 1u << i;
   });
   links[nid] = L;
+  const bool open = (x == 0 && open_lo) || (x == nx - 1 && open_hi);
   flags[nid] = solid ? FLAG_SOLID
-                     : (uint8_t)(((L >> 1) ? FLAG_BOUNDARY : 0) | (to_solid ? FLAG_SOLID_LINK : 0));
+                     : (uint8_t)(((L >> 1) ? FLAG_BOUNDARY : 0) | (to_solid ? FLAG_SOLID_LINK : 0) |
+                                 (open ? FLAG_OPEN : 0));
 }
 
 }  // namespace
@@ -138,8 +141,10 @@ int cons_blocks(size_t n) { return grid_for(n, CONS_THREADS); }
 cudaError_t classify(const Ctx& c, const int per[3], cudaStream_t s) {
   const dim3 b(32, 4, 2);
   const dim3 g((c.d.nx + 31) / 32, (c.d.ny + 3) / 4, (c.d.nz + 1) / 2);
-  k_classify<<<g, b, 0, s>>>(c.d.nx, c.d.ny, c.d.nz, per[0], per[1], per[2], c.mask, c.flags,
-                             c.links);
+  const bool phys = c.d.mode == LBM_MODE_PHYSICS;
+  k_classify<<<g, b, 0, s>>>(c.d.nx, c.d.ny, c.d.nz, per[0], per[1], per[2],
+                             phys && c.d.open_x[0] != LBM_OPEN_NONE, phys && c.d.open_x[1] != LBM_OPEN_NONE,
+                             c.mask, c.flags, c.links);
   return cudaGetLastError();
 }
 
