@@ -169,7 +169,10 @@ bool setup_physics(Ctx& c, const lbm_desc& d) {
   for (int f = 0; f < 6; ++f)
     for (int a = 0; a < 3; ++a) {
       p.wall[f][a] = d.wall_velocity[f][a];
-      if (d.wall_velocity[f][a] != 0.f) p.any_moving_wall = 1;
+      // an open face's velocity is the inlet's (the face kernel rebuilds
+      // every link across it), not a moving wall's
+      const bool open = f < 2 && d.open_x[f] != LBM_OPEN_NONE;
+      if (d.wall_velocity[f][a] != 0.f && !open) p.any_moving_wall = 1;
     }
   p.any_open = 0;
   for (int s = 0; s < 2; ++s) {

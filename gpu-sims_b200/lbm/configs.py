@@ -1,10 +1,14 @@
 """Workload definitions of the BASELINE configurations and the ensemble run.
 
     python -m lbm.configs ensemble [--steps 2000] [--domains 256]
+    python -m lbm.configs voxel
+    python -m lbm.configs duct [--steps 1000]
 
-(run from gpu-sims_b200/, or with it on sys.path) prints one JSON line: the
-aggregate MLUPS of the 256-cavity ensemble in fp16 and fp32 storage and the
-per-domain fp16-vs-fp32 velocity error.  All inputs are synthetic and seeded;
+(run from gpu-sims_b200/, or with it on sys.path) prints one JSON line:
+ensemble: the aggregate MLUPS of the 256-cavity ensemble in fp16 and fp32
+storage and the per-domain fp16-vs-fp32 velocity error; voxel: host against
+device NACA voxeliser at the capture tier; duct: the open-face channel
+(Zou-He inlet / outlet) against the walled one.  All inputs are synthetic and seeded;
 device time is measured with CUDA events on the library's stream.  The FP64
 comparisons of the cavity, Taylor-Green and channel workloads are GPU tests
 (tests/test_configs_gpu.py).
@@ -112,13 +116,87 @@ def tgv_init(N, u0=0.05):
     return rho.reshape(-1), u
 
 
+def run_voxel(shape=(512, 256, 256), preset=2, reps=5):
+    """The NACA mask of a preset at the capture tier: host voxeliser (one
+    core) against the device voxeliser, and set_flags(host mask) against
+    set_flags_naca (mask made on the device), each the median of reps."""
+    import torch
+    stream, timed = _timer()
+    p = lbm.PRESETS[preset]
+    nx, ny, nz = shape
+    n = nx * ny * nz
+    args = (lbm.AIRFOIL_CHORD_LENGTH_FRAC, lbm.AIRFOIL_CHORD_CENTER_X_FRAC, p.angle_of_attack_deg)
+    host_s = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        mask = lbm.voxelize_naca(p.naca, nx, ny, nz, *args)
+        host_s.append(time.perf_counter() - t0)
+    d = torch.empty(n, dtype=torch.uint8, device="cuda")
+    dev_s = [timed(lambda: lbm.voxelize_naca_device(p.naca, nx, ny, nz, d.data_ptr(), n, *args,
+                                                    stream=stream.cuda_stream)) for _ in range(reps + 1)][1:]
+    same = bool(np.array_equal(d.cpu().numpy(), mask))
+    lat = lbm.Lattice(nx=nx, ny=ny, nz=nz)
+    lat.set_stream(stream.cuda_stream)
+    up_s, naca_s = [], []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        lat.set_flags(mask)
+        up_s.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        lat.set_flags_naca(p.naca, *args)
+        naca_s.append(time.perf_counter() - t0)
+    lat.close()
+    med = lambda v: float(np.median(v))
+    return {"config": "voxel", "shape": list(shape), "naca": p.naca, "mask_bytes": n,
+            "host_voxelize_s": med(host_s), "device_voxelize_s": med(dev_s),
+            "speedup": med(host_s) / med(dev_s), "same_mask": same,
+            "set_flags_host_mask_s": med(up_s), "set_flags_naca_s": med(naca_s)}
+
+
+def run_duct(steps=1000, shape=(512, 128, 128)):
+    """Open-face channel: velocity inlet (u = 0.05) at x = 0, pressure outlet
+    (rho = 1) at x = nx-1, half-way bounce-back y / z walls, sphere r = 16 at
+    (128, 64, 64), tau = 0.55, BGK; MLUPS in fp32 and fp16 storage against the
+    same channel with walls in place of the open faces."""
+    stream, timed = _timer()
+    nx, ny, nz = shape
+    z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    mask = (((x - 128) ** 2 + (y - 64) ** 2 + (z - 64) ** 2) <= 256).astype(np.uint8).reshape(-1)
+    out = {"config": "duct", "shape": list(shape), "steps": steps}
+    for name, prec in (("f32", lbm.PREC_F32), ("f16s", lbm.PREC_F16S)):
+        for tag, kinds in (("open", (lbm.OPEN_VELOCITY, lbm.OPEN_PRESSURE)), ("walls", (0, 0))):
+            wall = np.zeros((6, 3))
+            if kinds[0]:
+                wall[lbm.FACE_XM] = (0.05, 0.0, 0.0)
+            d = lbm.default_desc(nx=nx, ny=ny, nz=nz, mode=lbm.MODE_PHYSICS, precision=prec, tau=0.55,
+                                 wall_velocity=wall, open_x=kinds, open_rho=(0.0, 1.0 if kinds[1] else 0.0))
+            lat = lbm.Lattice(d)
+            lat.set_stream(stream.cuda_stream)
+            lat.set_flags(mask)
+            lat.init_equilibrium(1.0, (0.0, 0.0, 0.0))
+            lat.step(20)
+            secs = timed(lambda: lat.step(steps))
+            lat.sync()
+            rho, u = lat.read_moments()
+            out[f"{name}_{tag}"] = {"mlups": nx * ny * nz * steps / secs / 1e6,
+                                    "finite": bool(np.isfinite(u).all()),
+                                    "outlet_mean_ux": float(u[:, 0].reshape(nz, ny, nx)[:, :, nx - 1].mean())}
+            lat.close()
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("config", choices=["ensemble"])
+    ap.add_argument("config", choices=["ensemble", "voxel", "duct"])
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--domains", type=int, default=256)
     a = ap.parse_args(argv)
-    r = run_ensemble(steps=a.steps or 2000, n=a.domains)
+    if a.config == "ensemble":
+        r = run_ensemble(steps=a.steps or 2000, n=a.domains)
+    elif a.config == "voxel":
+        r = run_voxel()
+    else:
+        r = run_duct(steps=a.steps or 1000)
     print(json.dumps(r), flush=True)
     return 0
 
