@@ -46,9 +46,11 @@ int validate(const lbm_desc* d) {
   if (!d) return fail(nullptr, LBM_ERR_INVALID_ARG, "desc is NULL");
   if (d->struct_size != sizeof(lbm_desc))
     return fail(nullptr, LBM_ERR_INVALID_ARG, "desc.struct_size does not match this library's lbm_desc");
-  const long long lim = 1 << 16;
+  // 65535: the largest grid y / z extent of a launch (rows and planes map to
+  // blockIdx.y / blockIdx.z)
+  const long long lim = 65535;
   if (d->nx < 2 || d->ny < 2 || d->nz < 2 || d->nx > lim || d->ny > lim || d->nz > lim)
-    return fail(nullptr, LBM_ERR_INVALID_ARG, "grid extents must be in [2, 65536]");
+    return fail(nullptr, LBM_ERR_INVALID_ARG, "grid extents must be in [2, 65535]");
   const double nodes = (double)d->nx * d->ny * d->nz;
   if (nodes > 4.0e9) return fail(nullptr, LBM_ERR_INVALID_ARG, "more than 4e9 nodes");
   if (d->mode != LBM_MODE_REFERENCE && d->mode != LBM_MODE_PHYSICS)

@@ -90,7 +90,7 @@ enum lbm_face { LBM_FACE_XM = 0, LBM_FACE_XP, LBM_FACE_YM, LBM_FACE_YP,
 /* ---- descriptor -------------------------------------------------------- */
 typedef struct lbm_desc {
     uint32_t struct_size;       /* sizeof(lbm_desc), for ABI growth          */
-    int32_t  nx, ny, nz;        /* lattice nodes; each >= 2                  */
+    int32_t  nx, ny, nz;        /* lattice nodes; each in [2, 65535]         */
     int32_t  mode;              /* enum lbm_mode                             */
     int32_t  precision;         /* enum lbm_precision                        */
     int32_t  collision;         /* enum lbm_collision (physics mode)         */
