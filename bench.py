@@ -359,8 +359,10 @@ def run_ours(args, world, rank, local):
         "roofline": {"bound": "hbm", "achieved": head["achieved_gbs"], "peak": peak, "unit": "GB/s",
                      "frac": head["frac"], "traffic": traffic,
                      "bytes_per_node": head["bytes_per_node"],
-                     "peak_kind": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)",
-                     "kernel": "k_phys_step (fused esoteric-pull stream+collide)"},
+                     "peak_kind": ("measured copy bandwidth (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                                   else "fallback copy bandwidth (6650 GB/s, an earlier measurement on this pool; "
+                                        "MEASURED_PEAKS.json absent)"),
+                     "kernel": "k_phys_step2 (fused esoteric-pull stream+collide, two nodes per thread)"},
         "variants": runs,
         "e2e": e2e,
         "gpu_launches": args.steps,
