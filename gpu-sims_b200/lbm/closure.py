@@ -1,6 +1,6 @@
 """Learned sub-grid closure: decaying homogeneous isotropic turbulence (HIT),
 the fine plain-LBM run that generates training data, the trainer and the
-coarse runs it is judged on.
+coarse runs it is evaluated on.
 
     python -m lbm.closure run [--fine 512] [--factor 4] [--snapshots 2000] ...
 

@@ -1,4 +1,5 @@
-"""Workload definitions of the BASELINE configurations and the ensemble run.
+"""Workload definitions of the benchmark configurations (lid-driven cavity,
+Taylor-Green vortex, channel, cavity ensemble) and the voxel and duct runs.
 
     python -m lbm.configs ensemble [--steps 2000] [--domains 256]
     python -m lbm.configs voxel
