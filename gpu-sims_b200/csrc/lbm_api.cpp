@@ -127,8 +127,7 @@ void free_all(Ctx* c) {
   for (auto& g : c->graph)
     if (g) cudaGraphExecDestroy(g);
   void* ptrs[] = {c->fbuf[0], c->fbuf[1], c->pop,      c->mask,     c->flags, c->links,
-                  c->rho,     c->u,       c->status,   c->partials, c->sums,  c->staging,
-                  c->pp.cons};
+                  c->rho,     c->u,       c->status,   c->partials, c->sums,  c->staging};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -275,12 +274,6 @@ int lbm_create(const lbm_desc* desc, lbm_ctx** out) {
       (rc = dev_alloc(c, &c->partials, 4 * (size_t)c->nblk_cons, "cudaMalloc(partials)")) ||
       (rc = dev_alloc(c, &c->sums, 4, "cudaMalloc(sums)")))
     return bail(rc);
-  if (desc->mode == LBM_MODE_PHYSICS) {
-    // per-warp fp64 conservation partials of the moment-writing launch
-    c->pp.cons_n = lbm::phys_cons_slots(c->pp.g);
-    if ((rc = dev_alloc(c, &c->pp.cons, 4 * (size_t)c->pp.cons_n, "cudaMalloc(conservation partials)")))
-      return bail(rc);
-  }
 
   cudaStream_t s = c->stream;
   if (c->fbuf[0]) {
@@ -420,7 +413,6 @@ static int do_init(lbm_ctx* c, const float* d_rho, const float* d_u, float rho0,
   CK(cudaMemsetAsync(c->status, 0, sizeof(unsigned), c->stream), "reset status");
   c->iteration = 0;
   c->initialized = true;
-  c->cons_fused = false;  // the init wrote the moments
   return LBM_OK;
 }
 
@@ -502,9 +494,6 @@ int lbm_step(lbm_ctx* c, int nsteps) {
     cudaError_t e = launch_one(c, i == left - 1, c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "step kernel launch");
   }
-  // the parity flipped with each launch; the layout depends on none of it
-  if (nsteps > 0)
-    c->cons_fused = c->d.mode == LBM_MODE_PHYSICS && lbm::phys_cons_layout(*c, &c->cons_rows, &c->cons_faces);
   c->iteration += (uint64_t)nsteps;
   return LBM_OK;
 }
@@ -551,12 +540,7 @@ int lbm_conservation(lbm_ctx* c, double out[4]) {
   if (int rc = check_ctx(c)) return rc;
   if (!out) return fail(c, LBM_ERR_INVALID_ARG, "out is NULL");
   if (!c->initialized) return fail(c, LBM_ERR_STATE, "conservation before lbm_init_*");
-  // after a physics step: the partials its moment-writing launch left;
-  // otherwise a pass over the moment arrays
-  if (c->cons_fused)
-    CK(lbm::conservation_fused(*c, c->stream), "conservation kernel");
-  else
-    CK(lbm::conservation_partials(*c, c->stream), "conservation kernels");
+  CK(lbm::conservation_partials(*c, c->stream), "conservation kernels");
   CK(cudaMemcpyAsync(out, c->sums, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream), "read sums");
   CK(cudaStreamSynchronize(c->stream), "conservation sync");
   return LBM_OK;

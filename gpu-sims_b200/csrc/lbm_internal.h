@@ -75,11 +75,6 @@ struct PhysParams {
   int open[2];
   float open_rho[2];
   int any_open;
-  // fp64 conservation partials of the moment-writing launch, one slot per
-  // warp in four planes of cons_n (rho, rho ux, rho uy, rho uz); null in
-  // batches
-  double* cons;
-  uint32_t cons_n;
 };
 
 struct Ctx;
@@ -113,13 +108,6 @@ cudaError_t phys_write_pops(const Ctx& c, const float* in, cudaStream_t s, bool 
 cudaError_t classify(const Ctx& c, const int per[3], cudaStream_t s);
 int cons_blocks(size_t n);
 cudaError_t conservation_partials(const Ctx& c, cudaStream_t s);
-// Conservation sums from the fused per-warp partials (c.cons_fused).
-cudaError_t conservation_fused(const Ctx& c, cudaStream_t s);
-// Warp slots the physics step's partials need (rows of the one-node path
-// plus both faces), and whether the step as configured writes them (rows /
-// faces: the slots its moment-writing launch fills).
-uint32_t phys_cons_slots(const PhysGeom& g);
-bool phys_cons_layout(const Ctx& c, uint32_t* rows, uint32_t* faces);
 cudaError_t u_planes_to_format(const float* u, size_t n, int fmt, void* out, cudaStream_t s);
 cudaError_t u_format_to_planes(const void* in, size_t n, int fmt, float* u, cudaStream_t s);
 
@@ -159,10 +147,6 @@ struct Ctx {
   float clo[LBM_CLOSURE_FLOATS] = {};
   // nodes per thread of the physics step: 0 automatic, 1, 2 or 4
   int step_variant = 0;
-  // the last moment-writing step also wrote fp64 conservation partials
-  // (pp.cons): warp slots [0, cons_rows) and the last cons_faces slots
-  bool cons_fused = false;
-  uint32_t cons_rows = 0, cons_faces = 0;
   bool initialized = false;
   uint64_t iteration = 0;
   uint64_t dev_bytes = 0;

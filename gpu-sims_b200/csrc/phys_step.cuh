@@ -347,27 +347,6 @@ __device__ __forceinline__ uint32_t offs(const PhysGeom& G, const Wrap& w) {
   return o;
 }
 
-// fp64 conservation partials of one warp (rho, rho ux, rho uy, rho uz of
-// the moments it writes, each product formed as the separate reduction over
-// the moment arrays forms it) into warp slot `slot`; every lane takes part.
-__device__ __forceinline__ void cons_warp(const PhysParams& p, uint32_t slot, double a, double b, double c,
-                                          double d) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    a += __shfl_down_sync(0xffffffffu, a, o);
-    b += __shfl_down_sync(0xffffffffu, b, o);
-    c += __shfl_down_sync(0xffffffffu, c, o);
-    d += __shfl_down_sync(0xffffffffu, d, o);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    double* q = p.cons + slot;
-    q[0] = a;
-    q[p.cons_n] = b;
-    q[2 * (size_t)p.cons_n] = c;
-    q[3 * (size_t)p.cons_n] = d;
-  }
-}
-
 // One fused stream+collide launch.  All lanes of a warp stay converged:
 //  * the 19 slots of the streaming pattern are loaded before the flag byte
 //    is known (a solid node's slots exist, so the loads are in bounds), so a
@@ -393,8 +372,7 @@ __device__ __forceinline__ void step_row(const PhysParams& p, const CloNet<SGS>&
                                          const uint32_t* __restrict__ links,
                                          float* __restrict__ rho_o, float* __restrict__ u_o,
                                          unsigned* __restrict__ status, const int x0, const int y,
-                                         const int z, const bool lane_ok = true,
-                                         const uint32_t cons_slot = 0) {
+                                         const int z, const bool lane_ok = true) {
   using S = Store<PREC>;
   using T = typename S::T;
   const PhysGeom& G = p.g;
@@ -503,13 +481,6 @@ __device__ __forceinline__ void step_row(const PhysParams& p, const CloNet<SGS>&
     if (fluid && (!(rho > 0.0f) || !isfinite(rho) || !isfinite(ux) || !isfinite(uy) || !isfinite(uz)))
       atomicOr(status, 1u);
   }
-  if constexpr (WRITE_MOMENTS && SGS != 3) {
-    if (p.cons) {  // uniform: set for single-domain launches
-      const double r = fluid ? (double)rho : 0.0;
-      cons_warp(p, cons_slot, r, fluid ? r * (double)ux : 0.0, fluid ? r * (double)uy : 0.0,
-                fluid ? r * (double)uz : 0.0);
-    }
-  }
 
   if (fluid) S::raw_st(pop, ln, g[0]);
   const bool pass = fluid && !edge;  // this lane's Y value is stored by lane+1
@@ -609,7 +580,7 @@ __device__ __forceinline__ void step_row2(const PhysParams& p, const CloNet<SGS>
                                           const uint32_t* __restrict__ links,
                                           float* __restrict__ rho_o, float* __restrict__ u_o,
                                           unsigned* __restrict__ status, const int x0, const int y,
-                                          const int z, const uint32_t cons_slot = 0) {
+                                          const int z) {
   using S = Store<PREC>;
   using V2 = Vec2<PREC>;
   using T = typename S::T;
@@ -712,15 +683,6 @@ __device__ __forceinline__ void step_row2(const PhysParams& p, const CloNet<SGS>
     const bool badB = fluidB && (!(r2.y > 0.f) || !isfinite(r2.y) || !isfinite(ux2.y) ||
                                  !isfinite(uy2.y) || !isfinite(uz2.y));
     if (badA || badB) atomicOr(status, 1u);
-  }
-  if constexpr (WRITE_MOMENTS) {
-    if (p.cons) {  // uniform: set for single-domain launches
-      const double ra = fluidA ? (double)r2.x : 0.0, rb = fluidB ? (double)r2.y : 0.0;
-      cons_warp(p, cons_slot, ra + rb,
-                (fluidA ? ra * (double)ux2.x : 0.0) + (fluidB ? rb * (double)ux2.y : 0.0),
-                (fluidA ? ra * (double)uy2.x : 0.0) + (fluidB ? rb * (double)uy2.y : 0.0),
-                (fluidA ? ra * (double)uz2.x : 0.0) + (fluidB ? rb * (double)uz2.y : 0.0));
-    }
   }
 
   const bool both = fluidA && fluidB;

@@ -50,9 +50,8 @@ __global__ void __launch_bounds__(32 * step2_rows<PREC, SGS>(),
   constexpr int R = step2_rows<PREC, SGS>();
   const int y = R == 1 ? (int)blockIdx.y : (int)(blockIdx.y * R + threadIdx.y);
   if (y >= p.g.ny) return;  // uniform over the warp
-  step_row2<PREC, COLL, SGS, FORCE, WRITE_MOMENTS, P>(
-      p, net, pop_v, flags, links, rho_o, u_o, status, blockIdx.x * 64, y, blockIdx.z,
-      ((uint32_t)blockIdx.z * (uint32_t)p.g.ny + (uint32_t)y) * gridDim.x + blockIdx.x);
+  step_row2<PREC, COLL, SGS, FORCE, WRITE_MOMENTS, P>(p, net, pop_v, flags, links, rho_o, u_o,
+                                                      status, blockIdx.x * 64, y, blockIdx.z);
 }
 
 template <int PREC, int COLL, int SGS, bool FORCE, bool WRITE_MOMENTS, int P>
@@ -63,9 +62,8 @@ __global__ void __launch_bounds__(STEP_THREADS, SGS == 2 ? LBM_CLO_MINB : LBM_ST
                 const __grid_constant__ CloNet<SGS> net) {
   const int y = blockIdx.y * STEP_BY + threadIdx.y;
   if (y >= p.g.ny) return;  // uniform over the warp
-  step_row<PREC, COLL, SGS, FORCE, WRITE_MOMENTS, P>(
-      p, net, pop_v, flags, links, rho_o, u_o, status, blockIdx.x * 32, y, blockIdx.z, true,
-      ((uint32_t)blockIdx.z * (uint32_t)p.g.ny + (uint32_t)y) * gridDim.x + blockIdx.x);
+  step_row<PREC, COLL, SGS, FORCE, WRITE_MOMENTS, P>(p, net, pop_v, flags, links, rho_o, u_o,
+                                                     status, blockIdx.x * 32, y, blockIdx.z);
 }
 
 // Open x faces: one thread per face node, lanes over (y, z), blockIdx.y
@@ -78,19 +76,13 @@ __global__ void __launch_bounds__(128)
                 float* __restrict__ u_o, unsigned* __restrict__ status,
                 const __grid_constant__ CloNet<SGS> net) {
   const int side = blockIdx.y;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  // warp slots of the conservation partials: the last 2 x (warps per side)
-  const uint32_t per_side = gridDim.x * (blockDim.x / 32);
-  const uint32_t slot = p.cons_n - 2 * per_side + (uint32_t)side * per_side + (uint32_t)t / 32;
-  if (p.open[side] == LBM_OPEN_NONE) {  // uniform over the block
-    if (WRITE_MOMENTS && p.cons) cons_warp(p, slot, 0.0, 0.0, 0.0, 0.0);
-    return;
-  }
+  if (p.open[side] == LBM_OPEN_NONE) return;  // uniform over the block
   const int nyz = p.g.ny * p.g.nz;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int tc = t < nyz ? t : nyz - 1;  // idle lanes take part in the shuffles
   step_row<PREC, COLL, SGS, FORCE, WRITE_MOMENTS, P, true>(p, net, pop_v, flags, links, rho_o, u_o,
                                                           status, side ? p.g.nx - 1 : 0, tc % p.g.ny,
-                                                          tc / p.g.ny, t < nyz, slot);
+                                                          tc / p.g.ny, t < nyz);
 }
 
 #ifndef LBM_STEP4_MINB

@@ -148,33 +148,6 @@ cudaError_t classify(const Ctx& c, const int per[3], cudaStream_t s) {
   return cudaGetLastError();
 }
 
-// Conservation sums from the step's per-warp partials: one block per
-// quantity, a fixed strided order and a fixed tree, so the result does not
-// depend on scheduling.
-__global__ void __launch_bounds__(1024) k_cons_fused(const double* __restrict__ cons, uint32_t n,
-                                                     uint32_t rows, uint32_t faces,
-                                                     double* __restrict__ out) {
-  const double* q = cons + (size_t)blockIdx.x * n;
-  double v = 0.0;
-  for (uint32_t i = threadIdx.x; i < rows; i += blockDim.x) v += q[i];
-  for (uint32_t i = threadIdx.x; i < faces; i += blockDim.x) v += q[n - faces + i];
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  __shared__ double sh[32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0) sh[warp] = v;
-  __syncthreads();
-  if (warp == 0) {
-    v = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (lane == 0) out[blockIdx.x] = v;
-  }
-}
-
-cudaError_t conservation_fused(const Ctx& c, cudaStream_t s) {
-  k_cons_fused<<<4, 1024, 0, s>>>(c.pp.cons, c.pp.cons_n, c.cons_rows, c.cons_faces, c.sums);
-  return cudaGetLastError();
-}
-
 cudaError_t conservation_partials(const Ctx& c, cudaStream_t s) {
   k_cons_partials<<<c.nblk_cons, CONS_THREADS, 0, s>>>(c.n, c.rho, c.u, c.partials, c.nblk_cons);
   k_cons_final<<<1, 128, 0, s>>>(c.partials, c.nblk_cons, c.sums);
