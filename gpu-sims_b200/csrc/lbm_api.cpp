@@ -546,6 +546,15 @@ int lbm_conservation(lbm_ctx* c, double out[4]) {
   return LBM_OK;
 }
 
+int lbm_conservation_async(lbm_ctx* c, double* out) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!out) return fail(c, LBM_ERR_INVALID_ARG, "out is NULL");
+  if (!c->initialized) return fail(c, LBM_ERR_STATE, "conservation before lbm_init_*");
+  CK(lbm::conservation_partials(*c, c->stream), "conservation kernels");
+  CK(cudaMemcpyAsync(out, c->sums, 4 * sizeof(double), cudaMemcpyDefault, c->stream), "copy sums");
+  return LBM_OK;
+}
+
 int lbm_read_populations(lbm_ctx* c, float* f, size_t n) {
   if (int rc = check_ctx(c)) return rc;
   if (!f || n != 19 * c->n) return fail(c, LBM_ERR_INVALID_ARG, "f must hold 19*Nx*Ny*Nz floats");

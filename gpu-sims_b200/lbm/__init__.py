@@ -135,6 +135,7 @@ _SIGS = {
     "lbm_destroy": (C.c_int, [_P]),
     "lbm_set_stream": (C.c_int, [_P, _P]),
     "lbm_set_flags": (C.c_int, [_P, _P, C.c_size_t]),
+    "lbm_conservation_async": (C.c_int, [_P, _P]),
     "lbm_set_flags_naca": (C.c_int, [_P, C.c_char_p, C.c_float, C.c_float, C.c_float]),
     "lbm_read_classification": (C.c_int, [_P, _P, C.c_size_t]),
     "lbm_init_equilibrium": (C.c_int, [_P, C.c_float, C.POINTER(C.c_float)]),
@@ -421,6 +422,11 @@ class Lattice:
         out = (C.c_double * 4)()
         self._c(load().lbm_conservation(self._h, out))
         return np.array(out[:], np.float64)
+
+    def conservation_async(self, out_ptr: int) -> None:
+        """Queue the sums into out_ptr (four doubles in pinned host or
+        device memory); valid once the stream reaches this point (sync)."""
+        self._c(load().lbm_conservation_async(self._h, C.c_void_p(out_ptr)))
 
     def read_populations(self) -> np.ndarray:
         f = np.empty((19, self.n), np.float32)

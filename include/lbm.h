@@ -208,6 +208,14 @@ LBM_API int lbm_device_moments(lbm_ctx* ctx, const float** d_rho, const float** 
 /* out[0] = sum rho, out[1..3] = sum rho*u over fluid nodes, in fp64. */
 LBM_API int lbm_conservation(lbm_ctx* ctx, double out[4]);
 
+/* lbm_conservation without the wait: queues the sums and their copy into
+ * out (pinned host or device memory, four doubles) on the context's stream
+ * and returns.  out holds the sums of the moments as they stand at this point
+ * of the stream once the stream gets there (lbm_sync, or an event); it must
+ * stay valid until then.  Lets a caller read every step's metric without
+ * stalling the step pipeline.  No counterpart in the reference. */
+LBM_API int lbm_conservation_async(lbm_ctx* ctx, double* out);
+
 /* Full population state, natural layout float[19][N] (direction-major),
  * post-collision populations of the current step.  For checkpoints. */
 LBM_API int lbm_read_populations(lbm_ctx* ctx, float* f, size_t n);

@@ -78,3 +78,26 @@ def test_fallback_paths(gpu):
     ref.step(3)
     check(ref, "reference mode")
     ref.close()
+
+
+def test_async_reads_equal_the_blocking_ones(gpu):
+    import torch
+    lat = flow(gpu, (64, 16, 12), periodic=(1, 0, 1), body_accel=(1e-5, 0, 0))
+    want = []
+    for _ in range(6):
+        lat.step(2)
+        want.append(lat.conservation())
+    lat2 = flow(gpu, (64, 16, 12), periodic=(1, 0, 1), body_accel=(1e-5, 0, 0))
+    host = torch.zeros((6, 4), dtype=torch.float64).pin_memory()
+    dev = torch.zeros((6, 4), dtype=torch.float64, device="cuda")
+    for i in range(6):
+        lat2.step(2)
+        lat2.conservation_async(host[i].data_ptr())
+        lat2.conservation_async(dev[i].data_ptr())
+    lat2.sync()
+    assert np.array_equal(host.numpy(), np.array(want))
+    assert np.array_equal(dev.cpu().numpy(), np.array(want))
+    with pytest.raises(gpu.LbmError):
+        lat2.conservation_async(0)
+    lat.close()
+    lat2.close()
