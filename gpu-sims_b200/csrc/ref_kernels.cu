@@ -92,14 +92,16 @@ __device__ __forceinline__ void set_equilibrium(float (&g)[Q], float rho, float 
   static_for<0, Q>([&](auto I) { g[I.value] = rl_feq<decltype(I)::value>(rho, ux, uy, uz, uu); });
 }
 
+// One warp per block, the row (y, z) from blockIdx: the row terms of the
+// pulls are warp-uniform to the compiler (uniform datapath).
 template <bool WRITE_MOMENTS>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(32, 32)
     k_ref_step(RefParams p, const float* __restrict__ fin, float* __restrict__ fout,
                const uint8_t* __restrict__ flags, const uint32_t* __restrict__ links,
                float* __restrict__ rho_o, float* __restrict__ u_o, unsigned* __restrict__ status) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z * blockDim.z + threadIdx.z;
+  const int x = blockIdx.x * 32 + threadIdx.x;
+  const int y = blockIdx.y;
+  const int z = blockIdx.z;
   if (x >= p.nx || y >= p.ny || z >= p.nz) return;
   const size_t N = p.n;
   const size_t nid = (size_t)x + (size_t)p.nx * ((size_t)y + (size_t)p.ny * (size_t)z);
@@ -234,6 +236,8 @@ dim3 ref_grid(const RefParams& p) {
   const dim3 b = ref_block();
   return dim3((p.nx + b.x - 1) / b.x, (p.ny + b.y - 1) / b.y, (p.nz + b.z - 1) / b.z);
 }
+// k_ref_step: one warp of 32 x per block, a block per (x tile, y, z)
+dim3 row_grid(const RefParams& p) { return dim3((p.nx + 31) / 32, p.ny, p.nz); }
 
 }  // namespace
 
@@ -249,11 +253,11 @@ cudaError_t ref_init(const Ctx& c, const float* rho, const float* u3, float rho0
 cudaError_t ref_step(const Ctx& c, const float* fin, float* fout, bool write_moments,
                      cudaStream_t s) {
   if (write_moments)
-    k_ref_step<true><<<ref_grid(c.rp), ref_block(), 0, s>>>(c.rp, fin, fout, c.flags, c.links,
-                                                            c.rho, c.u, c.status);
+    k_ref_step<true><<<row_grid(c.rp), 32, 0, s>>>(c.rp, fin, fout, c.flags, c.links, c.rho, c.u,
+                                                   c.status);
   else
-    k_ref_step<false><<<ref_grid(c.rp), ref_block(), 0, s>>>(c.rp, fin, fout, c.flags, c.links,
-                                                             c.rho, c.u, c.status);
+    k_ref_step<false><<<row_grid(c.rp), 32, 0, s>>>(c.rp, fin, fout, c.flags, c.links, c.rho, c.u,
+                                                    c.status);
   return cudaGetLastError();
 }
 
