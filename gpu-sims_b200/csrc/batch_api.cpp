@@ -180,7 +180,7 @@ size_t u_bytes(int fmt) {
 bool valid_schedule(const lbm_batch_schedule& s) {
   const bool rows = s.rows_per_block == 1 || s.rows_per_block == 2 || s.rows_per_block == 4 ||
                     s.rows_per_block == 8;
-  const bool z = s.z_per_thread >= 1 && s.z_per_thread <= 8;
+  const bool z = s.z_per_thread >= 1 && s.z_per_thread <= 16;
   return rows && z && (s.persistent == 0 || s.persistent == 1) && s.spin_limit_cycles > 0 &&
          s.test_missing_blocks >= 0;
 }
@@ -549,7 +549,7 @@ int lbm_batch_autotune(lbm_batch* b, int trial_steps, lbm_batch_schedule* best_o
   int rc = LBM_OK;
   for (int pers = 0; pers <= 1 && rc == LBM_OK; ++pers)
     for (int rows : {2, 4, 8})
-      for (int zt : {1, 2, 4}) {
+      for (int zt : {1, 2, 4, 8, 16}) {
         lbm_batch_schedule s = b->sched;
         s.rows_per_block = rows;
         s.z_per_thread = zt;

@@ -394,7 +394,7 @@ typedef struct lbm_batch lbm_batch;
 typedef struct lbm_batch_schedule {
     uint32_t struct_size;
     int32_t  rows_per_block;      /* 1, 2, 4, 8: a block is 32 x rows threads */
-    int32_t  z_per_thread;        /* 1..8 nodes along z per thread            */
+    int32_t  z_per_thread;        /* 1..16 nodes along z per thread           */
     int32_t  persistent;          /* 1 = one cooperative launch per call      */
     int64_t  spin_limit_cycles;   /* bound of a grid-barrier wait (persistent)*/
     int32_t  test_missing_blocks; /* testing only: barrier waits for this many

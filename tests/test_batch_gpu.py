@@ -63,7 +63,7 @@ def test_batch_equals_single_domains(gpu, prec, coll):
     steps = 37
     want = singles(gpu, descs, steps)
     for persistent in (0, 1):
-        for rows, zt in ((4, 1), (2, 2), (8, 4), (1, 3)):
+        for rows, zt in ((4, 1), (2, 2), (8, 4), (1, 3), (4, 8), (2, 16)):
             b = batch_of(gpu, descs)
             b.set_schedule(rows_per_block=rows, z_per_thread=zt, persistent=persistent)
             b.step(20)
@@ -109,7 +109,7 @@ def test_autotune_restores_state(gpu):
     b.step(5)
     before = [b.read_populations(i) for i in range(len(descs))]
     s = b.autotune(4)
-    assert s.rows_per_block in (2, 4, 8) and s.z_per_thread in (1, 2, 4)
+    assert s.rows_per_block in (2, 4, 8) and s.z_per_thread in (1, 2, 4, 8, 16)
     cur = b.schedule()
     assert (cur.rows_per_block, cur.z_per_thread, cur.persistent) == (s.rows_per_block, s.z_per_thread, s.persistent)
     for i in range(len(descs)):
