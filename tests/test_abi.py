@@ -41,7 +41,7 @@ def test_desc_validation_without_device(lbm_lib):
     bad = [dict(nx=1), dict(tau=0.5), dict(mode=7), dict(precision=9),
            dict(mode=lbm_lib.MODE_REFERENCE, precision=lbm_lib.PREC_F16S),
            dict(mode=lbm_lib.MODE_REFERENCE, periodic=(1, 0, 0)),
-           dict(ref_u_round=5)]
+           dict(ref_u_round=5), dict(nx=65536), dict(ny=70000, nx=2), dict(nz=-3)]
     for kw in bad:
         with pytest.raises(lbm_lib.LbmError) as e:
             lbm_lib.Lattice(**kw)
