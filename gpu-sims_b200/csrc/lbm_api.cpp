@@ -174,7 +174,7 @@ bool setup_physics(Ctx& c, const lbm_desc& d) {
       // an open face's velocity is the inlet's (the face kernel rebuilds
       // every link across it), not a moving wall's
       const bool open = f < 2 && d.open_x[f] != LBM_OPEN_NONE;
-      if (d.wall_velocity[f][a] != 0.f && !open) p.any_moving_wall = 1;
+      if (d.wall_velocity[f][a] != 0.f && !open) p.any_moving_wall |= 1 << f;
     }
   p.any_open = 0;
   for (int s = 0; s < 2; ++s) {

@@ -69,7 +69,7 @@ struct PhysParams {
   float smag_cs;
   float accel[3];
   float wall[6][3];
-  int any_moving_wall;
+  int any_moving_wall;  // bit f: face f (enum lbm_face) moves
   // open x faces (enum lbm_open; [0] = x-, [1] = x+): a VELOCITY face takes
   // its velocity from wall[0] / wall[1]
   int open[2];

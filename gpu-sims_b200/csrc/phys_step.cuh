@@ -347,6 +347,21 @@ __device__ __forceinline__ uint32_t offs(const PhysGeom& G, const Wrap& w) {
   return o;
 }
 
+// Moving-wall pass gate: a node gets momentum terms only through a link that
+// leaves through a moving face, so only nodes on such a face run the pass
+// (p.any_moving_wall holds bit f for each moving face f).  x_lo / x_hi are
+// the node group's first and last x.
+__device__ __forceinline__ bool near_moving(const PhysParams& p, int x_lo, int x_hi, int y, int z) {
+  const int m = p.any_moving_wall;
+  const PhysGeom& G = p.g;
+  return ((m & (1 << LBM_FACE_XM)) && !G.per[0] && x_lo == 0) ||
+         ((m & (1 << LBM_FACE_XP)) && !G.per[0] && x_hi == G.nx - 1) ||
+         ((m & (1 << LBM_FACE_YM)) && !G.per[1] && y == 0) ||
+         ((m & (1 << LBM_FACE_YP)) && !G.per[1] && y == G.ny - 1) ||
+         ((m & (1 << LBM_FACE_ZM)) && !G.per[2] && z == 0) ||
+         ((m & (1 << LBM_FACE_ZP)) && !G.per[2] && z == G.nz - 1);
+}
+
 // One fused stream+collide launch.  All lanes of a warp stay converged:
 //  * the 19 slots of the streaming pattern are loaded before the flag byte
 //    is known (a solid node's slots exist, so the loads are in bounds), so a
@@ -396,7 +411,7 @@ __device__ __forceinline__ void step_row(const PhysParams& p, const CloNet<SGS>&
   const bool xlo = !G.per[0] && xc == 0, xhi = !G.per[0] && xc == G.nx - 1;
   const bool ylo = !G.per[1] && y == 0, yhi = !G.per[1] && y == G.ny - 1;
   const bool zlo = !G.per[2] && z == 0, zhi = !G.per[2] && z == G.nz - 1;
-  const bool moving = p.any_moving_wall;
+  const bool moving = p.any_moving_wall && near_moving(p, xc, xc, y, z);
 
   const uint8_t fl = valid ? flags[nid] : FLAG_SOLID;
   float g[Q];
@@ -601,7 +616,7 @@ __device__ __forceinline__ void step_row2(const PhysParams& p, const CloNet<SGS>
   const bool xloA = !G.per[0] && xc == 0, xhiB = !G.per[0] && xc + 1 == G.nx - 1;
   const bool ylo = !G.per[1] && y == 0, yhi = !G.per[1] && y == G.ny - 1;
   const bool zlo = !G.per[2] && z == 0, zhi = !G.per[2] && z == G.nz - 1;
-  const bool moving = p.any_moving_wall;
+  const bool moving = p.any_moving_wall && near_moving(p, xc, xc + 1, y, z);
 
   const uint16_t fl2 = valid ? *reinterpret_cast<const uint16_t*>(flags + nid) : (uint16_t)0x0101u;
   const uint8_t flA = (uint8_t)(fl2 & 0xffu), flB = (uint8_t)(fl2 >> 8);
@@ -793,7 +808,7 @@ __device__ __forceinline__ void step_row4(const PhysParams& p, const CloNet<SGS>
   const bool xloA = !G.per[0] && xc == 0, xhiD = !G.per[0] && xc + 3 == G.nx - 1;
   const bool ylo = !G.per[1] && y == 0, yhi = !G.per[1] && y == G.ny - 1;
   const bool zlo = !G.per[2] && z == 0, zhi = !G.per[2] && z == G.nz - 1;
-  const bool moving = p.any_moving_wall;
+  const bool moving = p.any_moving_wall && near_moving(p, xc, xc + 3, y, z);
 
   const uint32_t fl4 = valid ? *reinterpret_cast<const uint32_t*>(flags + nid) : 0x01010101u;
   float2 gl[Q], gh[Q];  // gl: .x = A, .y = B;  gh: .x = C, .y = D
