@@ -411,7 +411,7 @@ __device__ __forceinline__ void step_row(const PhysParams& p, const CloNet<SGS>&
   const bool xlo = !G.per[0] && xc == 0, xhi = !G.per[0] && xc == G.nx - 1;
   const bool ylo = !G.per[1] && y == 0, yhi = !G.per[1] && y == G.ny - 1;
   const bool zlo = !G.per[2] && z == 0, zhi = !G.per[2] && z == G.nz - 1;
-  const bool moving = p.any_moving_wall && near_moving(p, xc, xc, y, z);
+  const bool moving = p.any_moving_wall;
 
   const uint8_t fl = valid ? flags[nid] : FLAG_SOLID;
   float g[Q];
@@ -442,7 +442,7 @@ __device__ __forceinline__ void step_row(const PhysParams& p, const CloNet<SGS>&
   });
   // Moving-wall momentum terms, in a pass of their own: inside the load loop
   // even a predicated-off add would wait for its load and serialise them.
-  if (moving) {
+  if (moving && near_moving(p, xc, xc, y, z)) {
     static_for<0, 9>([&](auto PI) {
       constexpr int pi = decltype(PI)::value;
       constexpr int a = pair_a(pi), b = pair_b(pi);
@@ -616,7 +616,7 @@ __device__ __forceinline__ void step_row2(const PhysParams& p, const CloNet<SGS>
   const bool xloA = !G.per[0] && xc == 0, xhiB = !G.per[0] && xc + 1 == G.nx - 1;
   const bool ylo = !G.per[1] && y == 0, yhi = !G.per[1] && y == G.ny - 1;
   const bool zlo = !G.per[2] && z == 0, zhi = !G.per[2] && z == G.nz - 1;
-  const bool moving = p.any_moving_wall && near_moving(p, xc, xc + 1, y, z);
+  const bool moving = p.any_moving_wall;
 
   const uint16_t fl2 = valid ? *reinterpret_cast<const uint16_t*>(flags + nid) : (uint16_t)0x0101u;
   const uint8_t flA = (uint8_t)(fl2 & 0xffu), flB = (uint8_t)(fl2 >> 8);
@@ -648,7 +648,7 @@ __device__ __forceinline__ void step_row2(const PhysParams& p, const CloNet<SGS>
       g2[b] = make_float2(V2::hi(yv), nxt);  // x + 1, x + 2
     }
   });
-  if (moving) {
+  if (moving && near_moving(p, xc, xc + 1, y, z)) {
     static_for<0, 9>([&](auto PI) {
       constexpr int pi = decltype(PI)::value;
       constexpr int a = pair_a(pi), b = pair_b(pi);
@@ -808,7 +808,7 @@ __device__ __forceinline__ void step_row4(const PhysParams& p, const CloNet<SGS>
   const bool xloA = !G.per[0] && xc == 0, xhiD = !G.per[0] && xc + 3 == G.nx - 1;
   const bool ylo = !G.per[1] && y == 0, yhi = !G.per[1] && y == G.ny - 1;
   const bool zlo = !G.per[2] && z == 0, zhi = !G.per[2] && z == G.nz - 1;
-  const bool moving = p.any_moving_wall && near_moving(p, xc, xc + 3, y, z);
+  const bool moving = p.any_moving_wall;
 
   const uint32_t fl4 = valid ? *reinterpret_cast<const uint32_t*>(flags + nid) : 0x01010101u;
   float2 gl[Q], gh[Q];  // gl: .x = A, .y = B;  gh: .x = C, .y = D
@@ -844,7 +844,7 @@ __device__ __forceinline__ void step_row4(const PhysParams& p, const CloNet<SGS>
       gh[b] = make_float2(yhi2.y, nxt);     // x + 3, x + 4
     }
   });
-  if (moving) {
+  if (moving && near_moving(p, xc, xc + 3, y, z)) {
     static_for<0, 9>([&](auto PI) {
       constexpr int pi = decltype(PI)::value;
       constexpr int a = pair_a(pi), b = pair_b(pi);
