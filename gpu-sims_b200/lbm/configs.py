@@ -1,7 +1,8 @@
 """Workload definitions of the benchmark configurations (lid-driven cavity,
 Taylor-Green vortex, channel, cavity ensemble) and the voxel and duct runs.
 
-    python -m lbm.configs ensemble [--steps 2000] [--domains 256]
+    python -m lbm.configs ensemble [--steps 2000] [--domains 256] [--precision f16s]
+                                   [--schedule rows,z,persistent]
     python -m lbm.configs voxel
     python -m lbm.configs duct [--steps 1000]
 
@@ -67,18 +68,26 @@ def ensemble_descs(n=256, seed=2024, precision=lbm.PREC_F16S, collision=lbm.COLL
     return descs, edges, res
 
 
-def run_ensemble(steps=2000, n=256, seed=2024, autotune=True, compare=True):
+def run_ensemble(steps=2000, n=256, seed=2024, autotune=True, compare=True, schedule=None,
+                 precisions=("f16s", "f32")):
+    """schedule: (rows, z, persistent) instead of the autotuner; precisions:
+    which storage runs (the fp16-vs-fp32 error needs both)."""
     stream, timed = _timer()
     out = {"config": "ensemble", "domains": n, "steps": steps}
     fields = {}
+    compare = compare and set(precisions) == {"f16s", "f32"}
     for name, prec in (("f16s", lbm.PREC_F16S), ("f32", lbm.PREC_F32)):
-        if name == "f32" and not compare:
-            break
+        if name not in precisions:
+            continue
         descs, edges, res = ensemble_descs(n, seed, prec)
         b = lbm.Batch(descs)
         b.set_stream(stream.cuda_stream)
         b.init_equilibrium(-1, 1.0, (0.0, 0.0, 0.0))
-        sched = b.autotune(10) if autotune else b.schedule()
+        if schedule is not None:
+            b.set_schedule(rows_per_block=schedule[0], z_per_thread=schedule[1], persistent=schedule[2])
+            sched = b.schedule()
+        else:
+            sched = b.autotune(10) if autotune else b.schedule()
         info = b.info()
         b.init_equilibrium(-1, 1.0, (0.0, 0.0, 0.0))
         secs = timed(lambda: b.step(steps))
@@ -191,9 +200,15 @@ def main(argv=None) -> int:
     ap.add_argument("config", choices=["ensemble", "voxel", "duct"])
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--domains", type=int, default=256)
+    ap.add_argument("--precision", choices=["both", "f16s", "f32"], default="both",
+                    help="ensemble: storage precisions to run")
+    ap.add_argument("--schedule", default=None,
+                    help="ensemble: rows,z,persistent instead of the autotuner (e.g. 4,16,0)")
     a = ap.parse_args(argv)
     if a.config == "ensemble":
-        r = run_ensemble(steps=a.steps or 2000, n=a.domains)
+        sched = tuple(int(v) for v in a.schedule.split(",")) if a.schedule else None
+        precs = ("f16s", "f32") if a.precision == "both" else (a.precision,)
+        r = run_ensemble(steps=a.steps or 2000, n=a.domains, schedule=sched, precisions=precs)
     elif a.config == "voxel":
         r = run_voxel()
     else:
