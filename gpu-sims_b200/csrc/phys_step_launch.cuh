@@ -111,8 +111,14 @@ __global__ void __launch_bounds__(STEP_THREADS, LBM_STEP4_MINB)
 #ifndef LBM_TC_ZPB
 #define LBM_TC_ZPB 8
 #endif
+// Two CTAs per SM: the kernel then keeps its 168 registers without spills
+// and runs 10.8 / 12.6 GLUPS (fp32 / fp16 storage, 128^3) against 9.0 / 9.7
+// at three CTAs per SM (spilling) and 10.2 / 11.2 for the CUDA-core MLP.
+#ifndef LBM_TC_MINB
+#define LBM_TC_MINB 2
+#endif
 template <int PREC, int COLL, bool WRITE_MOMENTS, int P>
-__global__ void __launch_bounds__(STEP_THREADS, LBM_CLO_MINB)
+__global__ void __launch_bounds__(STEP_THREADS, LBM_TC_MINB)
     k_phys_step_tc(PhysParams p, void* __restrict__ pop_v, const uint8_t* __restrict__ flags,
                    const uint32_t* __restrict__ links, float* __restrict__ rho_o,
                    float* __restrict__ u_o, unsigned* __restrict__ status,
@@ -278,10 +284,10 @@ cudaError_t launch_step_tc(const Ctx& c, int P, bool wm, cudaStream_t s) {
 
 // CLOSURE: the learned-closure kernels (compiled in their own files; no body
 // force, which lbm_set_closure enforces): the CUDA-core MLP (one or two
-// nodes per thread) by default, the tensor-core MLP for variant 8.  Measured
-// on B200 at 128^3 the CUDA-core pair kernel runs 10.4 GLUPS and the
-// tensor-core kernel 8.9: its per-plane CTA barrier around the MMA leaves the
-// memory latency of the next plane exposed.
+// nodes per thread, fp32 activations) by default, the tensor-core MLP (bf16
+// hidden activations) for variant 8.  Measured on B200 at 128^3: CUDA-core
+// pair kernel 10.2 / 11.2 GLUPS (fp32 / fp16 storage), tensor-core kernel
+// 10.8 / 12.6.
 template <int PREC, int COLL, bool CLOSURE>
 cudaError_t dispatch_smag(const Ctx& c, int P, bool wm, cudaStream_t s) {
   if constexpr (CLOSURE) {
