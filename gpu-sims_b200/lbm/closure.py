@@ -248,11 +248,12 @@ def apriori_loss(net: np.ndarray, fr: FineRun, stream=None) -> float:
     return loss
 
 
-def coarse_run(fr: FineRun, cs: float, net=None, stream=None):
+def coarse_run(fr: FineRun, cs: float, net=None, stream=None, step_variant: int = 0):
     """Coarse periodic BGK-Smagorinsky run (constant `cs`, or the learned
     closure with Cs^2 = cs^2 r when `net` is given) from the run's filtered
     initial field; device seconds of the steps, spectra and kinetic energy
-    every eval_every steps."""
+    every eval_every steps.  step_variant 8 evaluates the closure's hidden
+    layer on the tensor cores (bf16 activations)."""
     import torch
 
     import lbm
@@ -264,6 +265,8 @@ def coarse_run(fr: FineRun, cs: float, net=None, stream=None):
     lat.set_stream(stream.cuda_stream)
     if net is not None:
         lat.set_closure(net)
+        if step_variant:
+            lat.set_step_variant(step_variant)
     lat.init_from_moments(np.ascontiguousarray(fr.filt0[0]), np.ascontiguousarray(fr.filt0[1:4].T))
     secs, spectra, ke, ok = 0.0, {}, {}, True
     for s in range(0, fr.steps_c, fr.eval_every):
@@ -307,7 +310,8 @@ def run(fine: int = 512, factor: int = 4, tau_f: float = 0.508, snapshots: int =
         every: int = 8, samples_per_snapshot: int = 4096, cs0: float = 0.1, seed: int = 5,
         u_rms: float = 0.04, epochs: int = 20, batch: int = 4096, lr: float = 1e-3,
         eval_every: int = 250, kmax: int = 16,
-        calibrate=(0.1, 0.15, 0.2, 0.25, 0.35, 0.5, 0.75, 1.0, 1.5, 2.0), verbose: bool = True) -> dict:
+        calibrate=(0.1, 0.15, 0.2, 0.25, 0.35, 0.5, 0.75, 1.0, 1.5, 2.0), verbose: bool = True,
+        tensor_cores: bool = False) -> dict:
     """The experiment: a training run (seed) gives the samples and, by a
     sweep of a single scale on Cs0 against its own filtered spectra, the
     calibration of the learned closure; a held-out run (seed + 1) is the
@@ -317,6 +321,7 @@ def run(fine: int = 512, factor: int = 4, tau_f: float = 0.508, snapshots: int =
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     log = (lambda *a: print(*a, flush=True)) if verbose else (lambda *a: None)
+    variant = 8 if tensor_cores else 0  # step variant of the learned-closure coarse runs
     common = dict(fine=fine, factor=factor, tau_f=tau_f, snapshots=snapshots, every=every,
                   samples_per_snapshot=samples_per_snapshot, cs0=cs0, u_rms=u_rms,
                   eval_every=eval_every, stream=stream)
@@ -333,7 +338,7 @@ def run(fine: int = 512, factor: int = 4, tau_f: float = 0.508, snapshots: int =
     # calibration on the training run: one scale s on Cs0 (Cs^2 = s^2 cs0^2 r)
     cal = {}
     for a in calibrate:
-        e = errors(coarse_run(tr_run, cs0 * math.sqrt(a), net, stream), tr_run, kmax)
+        e = errors(coarse_run(tr_run, cs0 * math.sqrt(a), net, stream, variant), tr_run, kmax)
         cal[a] = e
         log(f"  calibration alpha {a}: time-mean err {e.get('time_mean')}")
     best = min((a for a in cal if cal[a]["finite"]), key=lambda a: cal[a]["time_mean"])
@@ -365,7 +370,7 @@ def run(fine: int = 512, factor: int = 4, tau_f: float = 0.508, snapshots: int =
     for name, cs, nn in (("smagorinsky", cs0, None), ("learned", cs0 * math.sqrt(best), net),
                          ("learned_uncalibrated", cs0, net),
                          ("smagorinsky_calibrated", cs0 * math.sqrt(best_s), None)):
-        e = errors(coarse_run(ev_run, cs, nn, stream), ev_run, kmax)
+        e = errors(coarse_run(ev_run, cs, nn, stream, variant if nn is not None else 0), ev_run, kmax)
         if e.get("device_s"):
             e["wall_ratio"] = ev_run.step_s / e["device_s"]
         res[name] = e
@@ -393,10 +398,12 @@ def main(argv=None) -> int:
     r.add_argument("--eval-every", type=int, default=250)
     r.add_argument("--seed", type=int, default=5)
     r.add_argument("--out", default=None, help="write the full results (with the network) here")
+    r.add_argument("--tensor-cores", action="store_true",
+                   help="learned-closure coarse runs with the hidden layer on the tensor cores")
     a = ap.parse_args(argv)
     res = run(fine=a.fine, factor=a.factor, tau_f=a.tau, snapshots=a.snapshots, every=a.every,
               samples_per_snapshot=a.samples, cs0=a.cs, epochs=a.epochs, batch=a.batch, lr=a.lr,
-              eval_every=a.eval_every, seed=a.seed)
+              eval_every=a.eval_every, seed=a.seed, tensor_cores=a.tensor_cores)
     if a.out:
         with open(a.out, "w") as f:
             json.dump(res, f)
