@@ -5,6 +5,7 @@ Taylor-Green vortex, channel, cavity ensemble) and the voxel and duct runs.
                                    [--schedule rows,z,persistent]
     python -m lbm.configs voxel
     python -m lbm.configs duct [--steps 1000]
+    python -m lbm.configs closure_step [--steps 200]
 
 (run from gpu-sims_b200/, or with it on sys.path) prints one JSON line:
 ensemble: the aggregate MLUPS of the 256-cavity ensemble in fp16 and fp32
@@ -195,9 +196,37 @@ def run_duct(steps=1000, shape=(512, 128, 128)):
     return out
 
 
+def run_closure_step(n=128, steps=200, variants=(0, 1, 8)):
+    """The learned-closure step on an n^3 periodic box (tau 0.502, Cs0 0.1, a
+    He-initialised network, seeded random velocity): MLUPS per step variant
+    (0 automatic: CUDA-core MLP, two nodes per thread; 1 one node per
+    thread; 8 tensor-core MLP) in fp32 and fp16 storage."""
+    from lbm import closure as cl
+    stream, timed = _timer()
+    net = cl.init_net(5, np.zeros(lbm.CLOSURE_INPUTS), np.ones(lbm.CLOSURE_INPUTS))
+    rng = np.random.default_rng(0)
+    u = (0.02 * rng.standard_normal((n ** 3, 3))).astype(np.float32)
+    out = {"config": "closure_step", "n": n, "steps": steps}
+    for name, prec in (("f32", lbm.PREC_F32), ("f16s", lbm.PREC_F16S)):
+        for v in variants:
+            d = lbm.default_desc(nx=n, ny=n, nz=n, mode=lbm.MODE_PHYSICS, precision=prec, periodic=(1, 1, 1),
+                                 tau=0.502, smagorinsky_cs=0.1)
+            lat = lbm.Lattice(d)
+            lat.set_stream(stream.cuda_stream)
+            lat.set_closure(net)
+            lat.init_from_moments(np.ones(n ** 3, np.float32), u)
+            lat.set_step_variant(v)
+            lat.step(20)
+            secs = timed(lambda: lat.step(steps))
+            lat.sync()
+            out[f"{name}_variant{v}"] = n ** 3 * steps / secs / 1e6
+            lat.close()
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("config", choices=["ensemble", "voxel", "duct"])
+    ap.add_argument("config", choices=["ensemble", "voxel", "duct", "closure_step"])
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--domains", type=int, default=256)
     ap.add_argument("--precision", choices=["both", "f16s", "f32"], default="both",
@@ -211,6 +240,8 @@ def main(argv=None) -> int:
         r = run_ensemble(steps=a.steps or 2000, n=a.domains, schedule=sched, precisions=precs)
     elif a.config == "voxel":
         r = run_voxel()
+    elif a.config == "closure_step":
+        r = run_closure_step(steps=a.steps or 200)
     else:
         r = run_duct(steps=a.steps or 1000)
     print(json.dumps(r), flush=True)
