@@ -500,7 +500,7 @@ int lbm_batch_read_populations(lbm_batch* b, int d, float* f, size_t n) {
 int lbm_batch_set_schedule(lbm_batch* b, const lbm_batch_schedule* s) {
   if (!b || !s) return bfail(b, LBM_ERR_INVALID_ARG, "NULL argument");
   if (s->struct_size != sizeof(lbm_batch_schedule) || !valid_schedule(*s))
-    return bfail(b, LBM_ERR_INVALID_ARG, "schedule out of range (rows 1/2/4/8, z 1..8, persistent 0/1)");
+    return bfail(b, LBM_ERR_INVALID_ARG, "schedule out of range (rows 1/2/4/8, z 1..16, persistent 0/1)");
   BCK(cudaStreamSynchronize(b->stream), "schedule sync");
   b->sched = *s;
   return build_tiles(b);

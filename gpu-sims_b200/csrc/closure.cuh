@@ -41,16 +41,27 @@ template <> struct CloNet<2> {
 // output layer on CUDA cores.  The first layer (9 -> 32) stays on CUDA
 // cores.  Built by k_phys_step_tc (phys_step_launch.cuh), which owns the
 // shared tiles, the mbarrier and the TMEM columns.
+//
+// A wait for an MMA that runs out (LBM_CLO_WAIT_LIMIT polls) must not leave
+// the tensor core reading a tile that the CTA goes on to rewrite.  So the A
+// tile is double-buffered by phase, a warp that gives up marks its entry of
+// `gave_up` (shared, sticky), and every later evaluation starts with a
+// __syncthreads_or over those marks: from then on the whole CTA issues no
+// MMA and falls back to r = 1, and the kernel drains the last commit (again
+// bounded) before it frees its tensor memory.
 template <> struct CloNet<3> {
   const CloNet<2>* net;     // parameters (kernel parameter space)
-  uint8_t* sA;              // A tile: 128 rows x 32 bf16, canonical K-major layout
+  uint8_t* sA;              // two A tiles: 128 rows x 32 bf16 each, canonical K-major layout
   uint32_t sA_addr, sB_addr, mbar_addr;  // shared-window addresses
   uint32_t tmem;            // TMEM base (lane 0, first column)
   unsigned* status;
+  uint32_t* gave_up;        // shared, one word per warp: that warp's wait ran out
+  uint32_t* last_phase;     // shared: phase of the last MMA commit issued
   bool row_ok;              // this thread's row exists (y < ny)
   uint32_t phase;           // mbarrier phase of this evaluation (alternates per use)
   __device__ __forceinline__ float operator[](int k) const { return net->v[k]; }
 };
+constexpr int CLO_TILE_A_BYTES = 128 * 64;
 
 // Shared-memory matrix descriptor of a K-major tile without swizzle: 8-row x
 // 16-byte core matrices, rows 16 B apart, K-adjacent core matrices `lbo`
@@ -151,20 +162,28 @@ __device__ __forceinline__ float closure_mlp_tc(const CloNet<3>& c, const float 
     const __nv_bfloat162 h = __floats2bfloat162_rn(fmaxf(a0, 0.f), fmaxf(a1, 0.f));
     hp[i / 2] = *reinterpret_cast<const uint32_t*>(&h);
   }
-  uint8_t* row = c.sA + clo_tile_off(r, 0);
+  // this warp's own mark (only it writes it): the same value in every lane
+  const bool warp_gave_up = c.gave_up[threadIdx.y] != 0;
+  const uint32_t buf = c.phase * CLO_TILE_A_BYTES;
+  uint8_t* row = c.sA + buf + clo_tile_off(r, 0);
+  if (!warp_gave_up) {
 #pragma unroll
-  for (int q = 0; q < 4; ++q)
-    *reinterpret_cast<uint4*>(row + q * 128) = make_uint4(hp[4 * q], hp[4 * q + 1], hp[4 * q + 2], hp[4 * q + 3]);
+    for (int q = 0; q < 4; ++q)
+      *reinterpret_cast<uint4*>(row + q * 128) =
+          make_uint4(hp[4 * q], hp[4 * q + 1], hp[4 * q + 2], hp[4 * q + 3]);
+  }
   // the A tile is visible to the tensor core, and every thread has finished
   // reading the previous evaluation's D, before the MMAs are issued
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  __syncthreads();
+  const bool abort = __syncthreads_or(warp_gave_up);  // uniform over the CTA
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (abort) return 1.0f;  // a wait ran out earlier in this launch: no more MMAs
   if (r == 0) {
+    *c.last_phase = c.phase;
 #pragma unroll
     for (int kk = 0; kk < 2; ++kk) {
-      const uint64_t da = clo_smem_desc(c.sA_addr + kk * 256, 128, 512);
+      const uint64_t da = clo_smem_desc(c.sA_addr + buf + kk * 256, 128, 512);
       const uint64_t db = clo_smem_desc(c.sB_addr + kk * 256, 128, 512);
       asm volatile(
           "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
@@ -182,7 +201,11 @@ __device__ __forceinline__ float closure_mlp_tc(const CloNet<3>& c, const float 
         : "=r"(done) : "r"(c.mbar_addr), "r"(c.phase) : "memory");
   // the tensor-memory load below is warp-collective: decide per warp
   if (!__all_sync(0xffffffffu, done != 0)) {  // gave up: plain Smagorinsky, error reported at sync
-    atomicOr(c.status, 2u);
+    if (threadIdx.x == 0) {
+      c.gave_up[threadIdx.y] = 1u;
+      atomicOr(c.status, 2u);
+    }
+    __syncwarp();
     return 1.0f;
   }
   __syncwarp();

@@ -198,6 +198,9 @@ double bytes_per_node(const lbm_desc& d) {
 
 extern "C" {
 
+static void drop_graphs(lbm_ctx* c);
+static int prepare_graphs(lbm_ctx* c);
+
 int lbm_desc_default(lbm_desc* d) {
   if (!d) return fail(nullptr, LBM_ERR_INVALID_ARG, "desc is NULL");
   std::memset(d, 0, sizeof(*d));
@@ -324,13 +327,9 @@ int lbm_set_step_variant(lbm_ctx* c, int nodes_per_thread) {
   if ((v == 4 || v == 8) && c->pp.any_open)
     return fail(c, LBM_ERR_UNSUPPORTED, "open x faces run with one or two nodes per thread");
   CK(cudaStreamSynchronize(c->stream), "set_step_variant sync");
-  for (auto& g : c->graph)
-    if (g) {
-      cudaGraphExecDestroy(g);
-      g = nullptr;
-    }
+  drop_graphs(c);
   c->step_variant = v;
-  return LBM_OK;
+  return c->initialized ? prepare_graphs(c) : LBM_OK;
 }
 
 int lbm_set_closure(lbm_ctx* c, const float* net) {
@@ -346,16 +345,12 @@ int lbm_set_closure(lbm_ctx* c, const float* net) {
   }
   // Captured step graphs hold the old network by value: rebuild them.
   CK(cudaStreamSynchronize(c->stream), "set_closure sync");
-  for (auto& g : c->graph)
-    if (g) {
-      cudaGraphExecDestroy(g);
-      g = nullptr;
-    }
+  drop_graphs(c);
   c->closure = net != nullptr;
   for (int k = 0; k < LBM_CLOSURE_FLOATS; ++k) {
     c->clo[k] = !net ? 0.f : lbm::clo_is_weight(k) ? lbm::round_bf16(net[k]) : net[k];
   }
-  return LBM_OK;
+  return c->initialized ? prepare_graphs(c) : LBM_OK;
 }
 
 // Classifies the mask already in c->mask (lbm_set_flags, lbm_set_flags_naca).
@@ -368,6 +363,8 @@ static int classify_mask(lbm_ctx* c) {
   // Physics mode keeps no populations at solid nodes, so a new mask needs a
   // new init; the reference step zeroes solids itself and can continue.
   if (c->d.mode == LBM_MODE_PHYSICS) c->initialized = false;
+  // the last step's boundaries used the old mask: it cannot be rerun
+  if (c->redo == Ctx::REDO_STEP) c->redo = Ctx::REDO_NONE;
   return LBM_OK;
 }
 
@@ -400,6 +397,65 @@ int lbm_read_classification(lbm_ctx* c, uint32_t* out, size_t n) {
   return LBM_OK;
 }
 
+// One step launch on stream s; flips the parity / current buffer.
+static cudaError_t launch_one(lbm_ctx* c, bool wm, cudaStream_t s) {
+  cudaError_t e;
+  if (c->d.mode == LBM_MODE_REFERENCE) {
+    e = lbm::ref_step(*c, c->fbuf[c->cur], c->fbuf[c->cur ^ 1], wm, s);
+    c->cur ^= 1;
+  } else {
+    e = lbm::phys_step(*c, c->parity, wm, s);
+    c->parity ^= 1;
+  }
+  return e;
+}
+
+// Captures kGraphSteps plain step launches, starting from the current parity,
+// on the context's own stream (a capture needs a non-legacy stream).  An even
+// count leaves the parity as it found it.
+static int build_graph(lbm_ctx* c, int slot) {
+  // capture from the slot's parity (current buffer); the captured launches do
+  // not run, and an even count brings the parity back, restored below anyway
+  int& par = c->d.mode == LBM_MODE_REFERENCE ? c->cur : c->parity;
+  const int saved = par;
+  par = slot;
+  struct Restore {
+    int& p;
+    int v;
+    ~Restore() { p = v; }
+  } restore{par, saved};
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(c->own_stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < Ctx::kGraphSteps && e == cudaSuccess; ++i) e = launch_one(c, false, c->own_stream);
+  cudaError_t e2 = cudaStreamEndCapture(c->own_stream, &g);
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return cuda_fail(c, e != cudaSuccess ? e : e2, "capture step graph");
+  }
+  e = cudaGraphInstantiate(&c->graph[slot], g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return cuda_fail(c, e, "instantiate step graph");
+  return LBM_OK;
+}
+
+static void drop_graphs(lbm_ctx* c) {
+  for (auto& g : c->graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+}
+
+// Builds the step graphs of both starting parities that do not exist yet, so
+// that no capture or instantiation falls inside a caller's step loop.
+static int prepare_graphs(lbm_ctx* c) {
+  for (int slot = 0; slot < 2; ++slot)
+    if (!c->graph[slot])
+      if (int rc = build_graph(c, slot)) return rc;
+  return LBM_OK;
+}
+
 static int do_init(lbm_ctx* c, const float* d_rho, const float* d_u, float rho0, const float* u0) {
   cudaError_t e;
   if (c->d.mode == LBM_MODE_REFERENCE) {
@@ -413,7 +469,8 @@ static int do_init(lbm_ctx* c, const float* d_rho, const float* d_u, float rho0,
   CK(cudaMemsetAsync(c->status, 0, sizeof(unsigned), c->stream), "reset status");
   c->iteration = 0;
   c->initialized = true;
-  return LBM_OK;
+  c->redo = Ctx::REDO_INIT;
+  return prepare_graphs(c);
 }
 
 int lbm_init_equilibrium(lbm_ctx* c, float rho0, const float u0[3]) {
@@ -444,38 +501,6 @@ int lbm_init_from_moments(lbm_ctx* c, const float* rho, const void* u, int u_fmt
   return LBM_OK;
 }
 
-// One step launch on stream s; flips the parity / current buffer.
-static cudaError_t launch_one(lbm_ctx* c, bool wm, cudaStream_t s) {
-  cudaError_t e;
-  if (c->d.mode == LBM_MODE_REFERENCE) {
-    e = lbm::ref_step(*c, c->fbuf[c->cur], c->fbuf[c->cur ^ 1], wm, s);
-    c->cur ^= 1;
-  } else {
-    e = lbm::phys_step(*c, c->parity, wm, s);
-    c->parity ^= 1;
-  }
-  return e;
-}
-
-// Captures kGraphSteps plain step launches, starting from the current parity,
-// on the context's own stream (a capture needs a non-legacy stream).  An even
-// count leaves the parity as it found it.
-static int build_graph(lbm_ctx* c, int slot) {
-  cudaGraph_t g = nullptr;
-  CK(cudaStreamBeginCapture(c->own_stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-  cudaError_t e = cudaSuccess;
-  for (int i = 0; i < Ctx::kGraphSteps && e == cudaSuccess; ++i) e = launch_one(c, false, c->own_stream);
-  cudaError_t e2 = cudaStreamEndCapture(c->own_stream, &g);
-  if (e != cudaSuccess || e2 != cudaSuccess) {
-    if (g) cudaGraphDestroy(g);
-    return cuda_fail(c, e != cudaSuccess ? e : e2, "capture step graph");
-  }
-  e = cudaGraphInstantiate(&c->graph[slot], g, 0);
-  cudaGraphDestroy(g);
-  if (e != cudaSuccess) return cuda_fail(c, e, "instantiate step graph");
-  return LBM_OK;
-}
-
 int lbm_step(lbm_ctx* c, int nsteps) {
   if (int rc = check_ctx(c)) return rc;
   if (nsteps < 0) return fail(c, LBM_ERR_INVALID_ARG, "nsteps must be >= 0");
@@ -483,16 +508,20 @@ int lbm_step(lbm_ctx* c, int nsteps) {
   int left = nsteps;
   // Whole graphs while more than kGraphSteps steps remain (the last launch
   // of the call must write the moments, so it is never inside a graph).
+  if (left > Ctx::kGraphSteps)
+    if (int rc = prepare_graphs(c)) return rc;
   while (left > Ctx::kGraphSteps) {
     const int slot = c->d.mode == LBM_MODE_REFERENCE ? c->cur : c->parity;
-    if (!c->graph[slot])
-      if (int rc = build_graph(c, slot)) return rc;
     CK(cudaGraphLaunch(c->graph[slot], c->stream), "graph launch");
     left -= Ctx::kGraphSteps;
   }
   for (int i = 0; i < left; ++i) {
     cudaError_t e = launch_one(c, i == left - 1, c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "step kernel launch");
+  }
+  if (nsteps > 0) {
+    c->redo = Ctx::REDO_STEP;
+    c->rp_last = c->rp;
   }
   c->iteration += (uint64_t)nsteps;
   return LBM_OK;
@@ -586,7 +615,8 @@ int lbm_write_populations(lbm_ctx* c, const float* f, size_t n) {
   }
   CK(cudaStreamSynchronize(c->stream), "write_populations sync");
   c->initialized = true;
-  return LBM_OK;
+  c->redo = Ctx::REDO_NONE;
+  return prepare_graphs(c);
 }
 
 int lbm_read_populations_shifted(lbm_ctx* c, float* g, size_t n) {
@@ -610,7 +640,8 @@ int lbm_write_populations_shifted(lbm_ctx* c, const float* g, size_t n) {
   CK(lbm::phys_write_pops(*c, static_cast<const float*>(c->staging), c->stream, true), "scatter populations");
   CK(cudaStreamSynchronize(c->stream), "write_populations_shifted sync");
   c->initialized = true;
-  return LBM_OK;
+  c->redo = Ctx::REDO_NONE;
+  return prepare_graphs(c);
 }
 
 int lbm_read_mask(lbm_ctx* c, uint8_t* mask, size_t n) {
@@ -650,6 +681,88 @@ int lbm_get_info(lbm_ctx* c, lbm_info* info) {
   info->layout = c->d.mode == LBM_MODE_PHYSICS ? 1 : 0;
   info->device = c->device;
   return LBM_OK;
+}
+
+int lbm_get_params(lbm_ctx* c, lbm_params* p) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!p || p->struct_size != sizeof(lbm_params))
+    return fail(c, LBM_ERR_INVALID_ARG, "params is NULL or params.struct_size is wrong");
+  const lbm_desc& d = c->d;
+  p->tau = d.tau;
+  std::memcpy(p->u_inf, d.u_inf, sizeof(p->u_inf));
+  std::memcpy(p->body_accel, d.body_accel, sizeof(p->body_accel));
+  std::memcpy(p->wall_velocity, d.wall_velocity, sizeof(p->wall_velocity));
+  p->smagorinsky_cs = d.smagorinsky_cs;
+  p->trt_magic = d.trt_magic;
+  std::memcpy(p->open_rho, d.open_rho, sizeof(p->open_rho));
+  return LBM_OK;
+}
+
+int lbm_set_params(lbm_ctx* c, const lbm_params* p) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!p || p->struct_size != sizeof(lbm_params))
+    return fail(c, LBM_ERR_INVALID_ARG, "params is NULL or params.struct_size is wrong");
+  lbm_desc d = c->d;
+  d.tau = p->tau;
+  std::memcpy(d.u_inf, p->u_inf, sizeof(d.u_inf));
+  std::memcpy(d.body_accel, p->body_accel, sizeof(d.body_accel));
+  std::memcpy(d.wall_velocity, p->wall_velocity, sizeof(d.wall_velocity));
+  d.smagorinsky_cs = p->smagorinsky_cs;
+  d.trt_magic = p->trt_magic;
+  std::memcpy(d.open_rho, p->open_rho, sizeof(d.open_rho));
+  for (int a = 0; a < 3; ++a)
+    if (!std::isfinite(d.u_inf[a]) || !std::isfinite(d.body_accel[a]))
+      return fail(c, LBM_ERR_INVALID_ARG, "u_inf and body_accel must be finite");
+  for (int f = 0; f < 6; ++f)
+    for (int a = 0; a < 3; ++a)
+      if (!std::isfinite(d.wall_velocity[f][a]))
+        return fail(c, LBM_ERR_INVALID_ARG, "wall velocities must be finite");
+  if (int rc = validate(&d)) return fail(c, rc, g_thread_err);
+  if (c->d.mode == LBM_MODE_REFERENCE) {
+    // The reference's uniforms carry tau and u_inf only (src/main.cpp:1523-1537).
+    if (std::memcmp(d.body_accel, c->d.body_accel, sizeof(d.body_accel)) ||
+        std::memcmp(d.wall_velocity, c->d.wall_velocity, sizeof(d.wall_velocity)) ||
+        d.trt_magic != c->d.trt_magic || std::memcmp(d.open_rho, c->d.open_rho, sizeof(d.open_rho)))
+      return fail(c, LBM_ERR_UNSUPPORTED, "reference mode takes tau and u_inf only");
+  } else if (c->closure) {
+    if (d.body_accel[0] != 0.f || d.body_accel[1] != 0.f || d.body_accel[2] != 0.f)
+      return fail(c, LBM_ERR_UNSUPPORTED, "the closure kernels are built without a body force");
+    if (!(d.smagorinsky_cs > 0.f))
+      return fail(c, LBM_ERR_INVALID_ARG, "the closure scales smagorinsky_cs, which must be > 0");
+  }
+  // Captured graphs and queued launches hold the old parameters by value.
+  CK(cudaStreamSynchronize(c->stream), "set_params sync");
+  drop_graphs(c);
+  const bool new_tau = d.tau != c->d.tau;
+  c->d = d;
+  if (d.mode == LBM_MODE_REFERENCE) {
+    // CollideUniforms / BoundariesUniforms as the host fills them
+    // (src/main.cpp:1524-1526, 1535).
+    c->rp.tau_inv = 1.0f / d.tau;
+    c->rp.omtau_inv = 1.0f - c->rp.tau_inv;
+    for (int a = 0; a < 3; ++a) c->rp.u_inf[a] = d.u_inf[a];
+    if (new_tau && c->initialized && c->redo != Ctx::REDO_NONE) {
+      // Recompute the pending collision with the new tau.
+      cudaError_t e;
+      if (c->redo == Ctx::REDO_INIT) {
+        // init's pre-collision state is feq of the moment fields it wrote
+        e = lbm::ref_init(*c, c->rho, c->u, 1.0f, nullptr, c->stream, false);
+      } else {
+        // rerun the last launch from its untouched input: boundaries with the
+        // parameters of that step, the collision with the new tau
+        lbm::RefParams q = c->rp_last;
+        q.tau_inv = c->rp.tau_inv;
+        q.omtau_inv = c->rp.omtau_inv;
+        e = lbm::ref_step_with(*c, q, c->fbuf[c->cur ^ 1], c->fbuf[c->cur], true, c->stream);
+        c->rp_last.tau_inv = q.tau_inv;
+        c->rp_last.omtau_inv = q.omtau_inv;
+      }
+      if (e != cudaSuccess) return cuda_fail(c, e, "recompute collision");
+    }
+  } else {
+    lbm::setup_physics(*c, d);
+  }
+  return c->initialized ? prepare_graphs(c) : LBM_OK;
 }
 
 const char* lbm_last_error(lbm_ctx* c) { return c ? c->err.c_str() : g_thread_err.c_str(); }

@@ -84,10 +84,16 @@ struct Ctx;
 bool step_pairs_host(int nx);
 
 // reference-mode kernels (ref_kernels.cu)
+// ref_init with write_moments = false leaves the moment fields alone (the
+// recomputation of the first collision from them after a tau change).
 cudaError_t ref_init(const Ctx& c, const float* rho, const float* u3, float rho0,
-                     const float* u0, cudaStream_t s);
+                     const float* u0, cudaStream_t s, bool write_moments = true);
 cudaError_t ref_step(const Ctx& c, const float* fin, float* fout, bool write_moments,
                      cudaStream_t s);
+// ref_step with explicit parameters (the boundaries of an earlier launch
+// with a new collision tau).
+cudaError_t ref_step_with(const Ctx& c, const RefParams& p, const float* fin, float* fout,
+                          bool write_moments, cudaStream_t s);
 
 // physics-mode kernels (phys_kernels.cu)
 cudaError_t phys_init(const Ctx& c, const float* rho, const float* u3, float rho0,
@@ -121,6 +127,14 @@ struct Ctx {
   float* fbuf[2] = {nullptr, nullptr};
   int cur = 0;
   RefParams rp{};
+  // What lbm_set_params must recompute after a tau change: the stored
+  // populations are the post-collision state of the next step, made by the
+  // init kernel (REDO_INIT: its inputs are the moment fields) or by the last
+  // step launch (REDO_STEP: its input is fbuf[cur ^ 1], its boundary
+  // parameters rp_last); REDO_NONE after a population write or a new mask.
+  enum { REDO_NONE = 0, REDO_INIT = 1, REDO_STEP = 2 };
+  int redo = REDO_NONE;
+  RefParams rp_last{};
   // physics mode: one esoteric-pull store
   void* pop = nullptr;
   int parity = 0;

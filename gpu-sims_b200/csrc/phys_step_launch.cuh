@@ -124,11 +124,15 @@ __global__ void __launch_bounds__(STEP_THREADS, LBM_TC_MINB)
                    float* __restrict__ u_o, unsigned* __restrict__ status,
                    const __grid_constant__ CloNet<2> net) {
   static_assert(STEP_THREADS == 128, "one MMA row per thread");
-  __shared__ __align__(1024) uint8_t sA[128 * 64];
+  __shared__ __align__(1024) uint8_t sA[2 * CLO_TILE_A_BYTES];
   __shared__ __align__(1024) uint8_t sB[CLO_HID * 64];
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tslot;
+  __shared__ uint32_t gave_up[STEP_THREADS / 32];
+  __shared__ uint32_t last_phase;
   const int tid = threadIdx.y * 32 + threadIdx.x;
+  if (tid < STEP_THREADS / 32) gave_up[tid] = 0u;
+  if (tid == 0) last_phase = 0u;
   for (int e = tid; e < CLO_HID * CLO_HID; e += STEP_THREADS)
     *reinterpret_cast<__nv_bfloat16*>(sB + clo_tile_off(e / CLO_HID, e % CLO_HID)) =
         __float2bfloat16_rn(net.v[CLO_W2 + e]);
@@ -154,6 +158,8 @@ __global__ void __launch_bounds__(STEP_THREADS, LBM_TC_MINB)
   c.mbar_addr = mbar_addr;
   c.tmem = tslot;
   c.status = status;
+  c.gave_up = gave_up;
+  c.last_phase = &last_phase;
   c.row_ok = y < p.g.ny;
   const int z0 = blockIdx.z * LBM_TC_ZPB;
   const int z1 = min(p.g.nz, z0 + LBM_TC_ZPB);  // uniform over the CTA
@@ -163,8 +169,19 @@ __global__ void __launch_bounds__(STEP_THREADS, LBM_TC_MINB)
                                                      blockIdx.x * 32, c.row_ok ? y : p.g.ny - 1, z);
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  __syncthreads();
+  const bool aborted = __syncthreads_or(gave_up[threadIdx.y] != 0);
   if (threadIdx.y == 0) {
+    if (aborted) {
+      // the last MMA whose wait ran out may still run: wait for its commit
+      // (bounded) before its tensor memory is freed
+      uint32_t done = 0;
+      for (int it = 0; it < LBM_CLO_WAIT_LIMIT && !done; ++it)
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}\n"
+            : "=r"(done) : "r"(mbar_addr), "r"(last_phase) : "memory");
+      __syncwarp();
+    }
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(c.tmem), "r"(32) : "memory");
   }

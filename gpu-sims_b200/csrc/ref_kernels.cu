@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(32, 32)
 __global__ void __launch_bounds__(256)
     k_ref_init(RefParams p, const float* __restrict__ rho_in, const float* __restrict__ u_in,
                float rho0, float u0x, float u0y, float u0z, float* __restrict__ fout,
-               float* __restrict__ rho_o, float* __restrict__ u_o) {
+               float* rho_o, float* u_o) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y * blockDim.y + threadIdx.y;
   const int z = blockIdx.z * blockDim.z + threadIdx.z;
@@ -225,10 +225,12 @@ __global__ void __launch_bounds__(256)
     const float feq = rl_feq<i>(r, qx, qy, qz, qq);
     fout[(size_t)i * N + nid] = rl_add(rl_mul(p.omtau_inv, f), rl_mul(p.tau_inv, feq));
   });
-  rho_o[nid] = r;
-  u_o[nid] = vx;
-  u_o[N + nid] = vy;
-  u_o[2 * N + nid] = vz;
+  if (rho_o) {
+    rho_o[nid] = r;
+    u_o[nid] = vx;
+    u_o[N + nid] = vy;
+    u_o[2 * N + nid] = vz;
+  }
 }
 
 dim3 ref_block() { return dim3(32, 4, 2); }
@@ -242,23 +244,27 @@ dim3 row_grid(const RefParams& p) { return dim3((p.nx + 31) / 32, p.ny, p.nz); }
 }  // namespace
 
 cudaError_t ref_init(const Ctx& c, const float* rho, const float* u3, float rho0, const float* u0,
-                     cudaStream_t s) {
+                     cudaStream_t s, bool write_moments) {
   const float zero[3] = {0.f, 0.f, 0.f};
   if (!u0) u0 = zero;
   k_ref_init<<<ref_grid(c.rp), ref_block(), 0, s>>>(c.rp, rho, u3, rho0, u0[0], u0[1], u0[2],
-                                                    c.fbuf[c.cur], c.rho, c.u);
+                                                    c.fbuf[c.cur], write_moments ? c.rho : nullptr,
+                                                    write_moments ? c.u : nullptr);
+  return cudaGetLastError();
+}
+
+cudaError_t ref_step_with(const Ctx& c, const RefParams& p, const float* fin, float* fout,
+                          bool write_moments, cudaStream_t s) {
+  if (write_moments)
+    k_ref_step<true><<<row_grid(p), 32, 0, s>>>(p, fin, fout, c.flags, c.links, c.rho, c.u, c.status);
+  else
+    k_ref_step<false><<<row_grid(p), 32, 0, s>>>(p, fin, fout, c.flags, c.links, c.rho, c.u, c.status);
   return cudaGetLastError();
 }
 
 cudaError_t ref_step(const Ctx& c, const float* fin, float* fout, bool write_moments,
                      cudaStream_t s) {
-  if (write_moments)
-    k_ref_step<true><<<row_grid(c.rp), 32, 0, s>>>(c.rp, fin, fout, c.flags, c.links, c.rho, c.u,
-                                                   c.status);
-  else
-    k_ref_step<false><<<row_grid(c.rp), 32, 0, s>>>(c.rp, fin, fout, c.flags, c.links, c.rho, c.u,
-                                                    c.status);
-  return cudaGetLastError();
+  return ref_step_with(c, c.rp, fin, fout, write_moments, s);
 }
 
 }  // namespace lbm

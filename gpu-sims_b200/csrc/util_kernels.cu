@@ -177,12 +177,12 @@ cudaError_t u_format_to_planes(const void* in, size_t n, int fmt, float* u, cuda
 // every GPU loading this library holds until the process exits.
 //
 // In host code `g_noalloc_scratch` names a host-side shadow, not device
-// memory, so its device address is looked up once per device with
-// cudaGetSymbolAddress (with that device current) and the kernels receive
-// that address.
+// memory, so every call looks its device address up with
+// cudaGetSymbolAddress (with the caller's device current; the lookup
+// allocates nothing) and the kernels receive that address.  Looking it up on
+// every call, rather than caching it, keeps the address right for whichever
+// context is current, also after a cudaDeviceReset reloaded the module.
 // ---------------------------------------------------------------------------
-#include <mutex>
-
 namespace lbm {
 void set_thread_error(const char* msg);
 }
@@ -191,11 +191,8 @@ namespace {
 constexpr int kNoAllocMaxBlocks = 4096;                 // partial-sum slots per quantity
 constexpr size_t kNoAllocNodesPerBlock = 8192;          // 256 threads x 32 nodes
 constexpr size_t kNoAllocMaxNodes = kNoAllocMaxBlocks * kNoAllocNodesPerBlock;  // 33,554,432
-constexpr int kNoAllocMaxDevices = 64;
 // 4 x 4096 partials + 4 sums, fp64: 131,104 bytes per device.
 static __device__ __align__(256) double g_noalloc_scratch[4 * kNoAllocMaxBlocks + 4];
-std::mutex g_noalloc_mu;
-double* g_noalloc_addr[kNoAllocMaxDevices] = {};
 }  // namespace
 
 extern "C" LBM_API int lbm_conservation_noalloc(const float* d_rho, const float* d_u, size_t n,
@@ -215,25 +212,14 @@ extern "C" LBM_API int lbm_conservation_noalloc(const float* d_rho, const float*
     lbm::set_thread_error("lbm_conservation_noalloc: no current CUDA device");
     return LBM_ERR_NO_DEVICE;
   }
-  if (dev < 0 || dev >= kNoAllocMaxDevices) {
-    lbm::set_thread_error("lbm_conservation_noalloc: device ordinal above 63");
-    return LBM_ERR_UNSUPPORTED;
+  void* p = nullptr;
+  const cudaError_t ea = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (ea != cudaSuccess || !p) {
+    cudaGetLastError();
+    lbm::set_thread_error("lbm_conservation_noalloc: cudaGetSymbolAddress failed");
+    return LBM_ERR_CUDA;
   }
-  double* scratch = nullptr;
-  {
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
-      void* p = nullptr;
-      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-      if (e != cudaSuccess || !p) {
-        cudaGetLastError();
-        lbm::set_thread_error("lbm_conservation_noalloc: cudaGetSymbolAddress failed");
-        return LBM_ERR_CUDA;
-      }
-      g_noalloc_addr[dev] = static_cast<double*>(p);
-    }
-    scratch = g_noalloc_addr[dev];
-  }
+  double* scratch = static_cast<double*>(p);
   // Every partial the final kernel reads is written first by its block, and
   // the sums are overwritten, so nothing needs clearing between calls.
   const int nblk = (int)((n + kNoAllocNodesPerBlock - 1) / kNoAllocNodesPerBlock);

@@ -75,6 +75,15 @@ class Info(C.Structure):
     ]
 
 
+class Params(C.Structure):
+    """lbm_params: solver parameters changeable between steps."""
+    _fields_ = [
+        ("struct_size", C.c_uint32), ("tau", C.c_float), ("u_inf", C.c_float * 3),
+        ("body_accel", C.c_float * 3), ("wall_velocity", (C.c_float * 3) * 6),
+        ("smagorinsky_cs", C.c_float), ("trt_magic", C.c_float), ("open_rho", C.c_float * 2),
+    ]
+
+
 class BatchSchedule(C.Structure):
     _fields_ = [
         ("struct_size", C.c_uint32),
@@ -97,6 +106,24 @@ class CaptureInfo(C.Structure):
         ("frame", C.c_uint32), ("iteration", C.c_uint64), ("has_populations", C.c_int32),
         ("mask_frame_invariant", C.c_int32),
     ]
+
+
+VDB_F32 = 1
+
+
+def vdb_write_vec3(path: str, xyz: np.ndarray, shape, voxel_size: float = 1.0, origin=None,
+                   grid_name: str | None = None) -> None:
+    """Writes a dense vec3 grid (xyz float[N][3], x-fastest) as an OpenVDB
+    file (lbm_vdb_write_vec3)."""
+    a = np.ascontiguousarray(xyz, dtype=np.float32).reshape(-1, 3)
+    nx, ny, nz = shape
+    if a.shape[0] != nx * ny * nz:
+        raise LbmError(ERR_INVALID_ARG, "xyz must hold Nx*Ny*Nz vectors")
+    org = None if origin is None else (C.c_float * 3)(*origin)
+    rc = load().lbm_vdb_write_vec3(str(path).encode(), _ptr(a), nx, ny, nz, voxel_size, org,
+                                   None if grid_name is None else grid_name.encode())
+    if rc != OK:
+        raise LbmError(rc, load().lbm_vdb_last_error().decode())
 
 
 CAPTURE_LOAD_MASK = 1
@@ -178,6 +205,8 @@ _SIGS = {
     "lbm_read_populations_shifted": (C.c_int, [_P, _P, C.c_size_t]),
     "lbm_write_populations_shifted": (C.c_int, [_P, _P, C.c_size_t]),
     "lbm_get_desc": (C.c_int, [_P, C.POINTER(Desc)]),
+    "lbm_get_params": (C.c_int, [_P, C.POINTER(Params)]),
+    "lbm_set_params": (C.c_int, [_P, C.POINTER(Params)]),
     "lbm_set_iteration": (C.c_int, [_P, _U64]),
     "lbm_capture_write": (C.c_int, [C.c_char_p, C.c_uint32, C.c_char_p, _I32, _I32, _I32, _P, _P, _P, _P]),
     "lbm_capture_read": (C.c_int, [C.c_char_p, C.POINTER(CaptureInfo), _P, _P, _P, _P]),
@@ -206,6 +235,9 @@ _SIGS = {
     "lbm_trainer_get_net": (C.c_int, [_P, _P]),
     "lbm_trainer_last_error": (C.c_char_p, [_P]),
     "lbm_round_bf16": (C.c_int, [_P, _P, C.c_size_t]),
+    "lbm_vdb_write_vec3": (C.c_int, [C.c_char_p, _P, _I32, _I32, _I32, _F, _P, C.c_char_p]),
+    "lbm_vdb_export": (C.c_int, [_P, C.c_char_p, C.c_uint32, C.c_int]),
+    "lbm_vdb_last_error": (C.c_char_p, []),
 }
 
 _lib = None
@@ -347,6 +379,40 @@ class Lattice:
     def write_populations_shifted(self, g: np.ndarray) -> None:
         a = np.ascontiguousarray(g, dtype=np.float32)
         self._c(load().lbm_write_populations_shifted(self._h, _ptr(a), a.size))
+
+    def params(self) -> Params:
+        p = Params()
+        p.struct_size = C.sizeof(Params)
+        self._c(load().lbm_get_params(self._h, C.byref(p)))
+        return p
+
+    def set_params(self, **kw) -> None:
+        """Changes solver parameters between steps (lbm_set_params), e.g.
+        set_params(tau=0.7, u_inf=(0.03, 0.0, 0.0)); unnamed fields keep their
+        current values."""
+        p = self.params()
+        for k, v in kw.items():
+            if k in ("u_inf", "body_accel", "open_rho"):
+                arr = getattr(p, k)
+                for i, x in enumerate(v):
+                    arr[i] = x
+            elif k == "wall_velocity":
+                for f, vec in enumerate(v):
+                    for a, x in enumerate(vec):
+                        p.wall_velocity[f][a] = x
+            elif k in ("tau", "smagorinsky_cs", "trt_magic"):
+                setattr(p, k, v)
+            else:
+                raise LbmError(ERR_INVALID_ARG, f"unknown parameter {k}")
+        self._c(load().lbm_set_params(self._h, C.byref(p)))
+
+    def vdb_export(self, directory: str, frame: int, f32: bool = False) -> str:
+        """Writes <directory>/velocity_<frame:06d>.vdb (lbm_vdb_export);
+        returns the path."""
+        rc = load().lbm_vdb_export(self._h, str(directory).encode(), frame, VDB_F32 if f32 else 0)
+        if rc != OK:
+            raise LbmError(rc, load().lbm_vdb_last_error().decode())
+        return str(Path(directory) / f"velocity_{frame:06d}.vdb")
 
     def set_step_variant(self, nodes_per_thread: int) -> None:
         self._c(load().lbm_set_step_variant(self._h, nodes_per_thread))

@@ -123,6 +123,23 @@ typedef struct lbm_info {
     int32_t  device;             /* CUDA ordinal                             */
 } lbm_info;
 
+/* Solver parameters that may change between lbm_step calls without touching
+ * the flow state (lbm_get_params / lbm_set_params).  The reference rebuilds
+ * CollideUniforms.tau_inv / omtau_inv and BoundariesUniforms.u_inf every frame
+ * (src/main.cpp:1523-1537) from its tau and |u_inf| / angle-of-attack sliders
+ * (src/main.cpp:1648, 1657-1661). */
+typedef struct lbm_params {
+    uint32_t struct_size;       /* sizeof(lbm_params)                        */
+    float    tau;               /* relaxation time (> 0.5)                   */
+    float    u_inf[3];          /* reference mode: inlet velocity            */
+    float    body_accel[3];     /* physics mode: Guo force, F = rho * accel  */
+    float    wall_velocity[6][3]; /* physics mode: per-face wall velocity
+                                   (open x faces: the inlet velocity)        */
+    float    smagorinsky_cs;    /* physics mode: 0 = off                     */
+    float    trt_magic;         /* physics mode: TRT Lambda                  */
+    float    open_rho[2];       /* physics mode: density of a PRESSURE face  */
+} lbm_params;
+
 typedef struct lbm_ctx lbm_ctx;
 
 /* Fills *d with the reference defaults: 64^3, reference mode, fp32, BGK,
@@ -187,6 +204,26 @@ LBM_API int lbm_step(lbm_ctx* ctx, int nsteps);
  * knob; LBM_ERR_UNSUPPORTED for a variant the grid or precision cannot use. */
 LBM_API int lbm_set_step_variant(lbm_ctx* ctx, int nodes_per_thread);
 
+/* The parameters in effect (from the descriptor, or the last lbm_set_params). */
+LBM_API int lbm_get_params(lbm_ctx* ctx, lbm_params* params);
+
+/* Changes the solver parameters between steps; populations, moments and the
+ * step counter are kept.  Replaces the per-frame uniform upload of
+ * src/main.cpp:1523-1537 driven by the sliders at :1648 and :1657-1661.
+ * The new values apply from the next collision and the next boundary pass,
+ * as a uniform upload before the next frame's dispatches does in the
+ * reference.  Reference mode: the stored state between launches is the
+ * post-collision population of the next step, so a tau change recomputes
+ * that collision with the new tau (one extra launch; bit-identical to the
+ * reference's four-pass step with the change made between frames).  After
+ * lbm_write_populations or an lbm_set_flags since the last step, the pending
+ * collision cannot be recomputed and keeps the old tau (the reference cannot
+ * be in that state).  Reference mode accepts only tau and u_inf (the other
+ * fields must equal the current ones); physics mode ignores u_inf.  The
+ * validation rules of lbm_create apply; with a learned closure installed,
+ * body_accel must stay 0 and smagorinsky_cs > 0. */
+LBM_API int lbm_set_params(lbm_ctx* ctx, const lbm_params* params);
+
 /* Waits for the context's stream; returns LBM_ERR_NONFINITE if a NaN/Inf or
  * non-positive density was seen at a fluid node since the last sync, and
  * LBM_ERR_TIMEOUT if a learned-closure step's bounded wait for its
@@ -240,11 +277,12 @@ LBM_API const char* lbm_last_error(lbm_ctx* ctx);
  * the device-wide synchronisation of cudaMalloc/cudaFree, or a host whose
  * memory arena owns the whole device budget.  Its scratch is a static
  * 131,104-byte device array that every GPU loading the library keeps until
- * exit; n is limited to 33,554,432 nodes (LBM_ERR_INVALID_ARG beyond).  The
- * first call on a device looks the array's address up for that device, so
- * make that first call before any stream capture.  All calls share the one
- * array: calls that overlap on the GPU race.  Runs on `stream` (NULL = the
- * legacy default stream) and synchronises it. */
+ * exit; n is limited to 33,554,432 nodes (LBM_ERR_INVALID_ARG beyond).  Every
+ * call looks the array's address up for the current device (no allocation).
+ * All calls share the one array: calls that overlap on the GPU race.  Runs on
+ * `stream` (NULL = the legacy default stream), copies the sums to pageable
+ * host memory and synchronises the stream, so it cannot be called while that
+ * stream (or the legacy stream) is being captured into a CUDA graph. */
 LBM_API int lbm_conservation_noalloc(const float* d_rho, const float* d_u, size_t n,
                                      double out[4], void* stream);
 
@@ -253,7 +291,8 @@ LBM_API int lbm_conservation_noalloc(const float* d_rho, const float* d_u, size_
  * (src/main.cpp:1296). */
 LBM_API int lbm_read_mask(lbm_ctx* ctx, uint8_t* mask, size_t n);
 
-/* The descriptor the context was created with. */
+/* The descriptor the context was created with, with the parameters of the
+ * last lbm_set_params. */
 LBM_API int lbm_get_desc(lbm_ctx* ctx, lbm_desc* desc);
 
 /* Sets the step counter reported by lbm_get_info (a capture resume restores
@@ -317,6 +356,28 @@ LBM_API int lbm_capture_save(lbm_ctx* ctx, const char* root, uint32_t frame,
  * iteration counter from the meta. */
 LBM_API int lbm_capture_load(lbm_ctx* ctx, const char* dir, int flags);
 LBM_API const char* lbm_capture_last_error(void);
+
+/* ---- VDB export --------------------------------------------------------- */
+/* The reference's optional VDB export (src/main.cpp:1767-1790) writes
+ * vdb_export/velocity_%06u.vdb through gpusims::vdb::writeVec3Grid
+ * (common/common-cpp/src/vdb_writer.cpp:96-141, which needs OpenVDB).  These
+ * write the same grid in the OpenVDB file layout (format version 224) with no
+ * OpenVDB dependency: a Vec3SGrid ("Tree_vec3s_5_4_3") named grid_name
+ * (NULL: "velocity"), class "staggered", linear transform of voxel_size (a
+ * translation by origin if origin is non-NULL and nonzero), every voxel of
+ * the Nx x Ny x Nz box active and stored in a leaf, values uncompressed.
+ * xyz: float[N][3], x-fastest.  LBM_ERR_IO when the file cannot be written;
+ * lbm_vdb_last_error gives the message. */
+LBM_API int lbm_vdb_write_vec3(const char* path, const float* xyz, int32_t nx, int32_t ny,
+                               int32_t nz, float voxel_size, const float origin[3],
+                               const char* grid_name);
+#define LBM_VDB_F32 1  /* the fp32 velocity instead of its rgba16f rounding */
+/* The frame-loop export: reads the lattice's velocity as the reference does
+ * (rgba16f, then half -> float; with LBM_VDB_F32 the fp32 field itself) and
+ * writes <dir>/velocity_<frame_idx, 6 digits>.vdb with voxel size 1 at the
+ * origin, grid "velocity". */
+LBM_API int lbm_vdb_export(lbm_ctx* ctx, const char* dir, uint32_t frame_idx, int flags);
+LBM_API const char* lbm_vdb_last_error(void);
 
 /* ---- streamlines ------------------------------------------------------- */
 /* Streamline advection over the device velocity field, the reference's

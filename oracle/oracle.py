@@ -14,8 +14,12 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
+# the same source built for speed (-O3, FMA contraction, AVX2): only the timed
+# CPU baseline uses it; parity always uses LIB
+LIB_FAST = HERE / "liboracle_fast.so"
 
 _lib = None
+_lib_fast = None
 _P = C.c_void_p
 
 
@@ -24,36 +28,45 @@ def build() -> Path:
     return LIB
 
 
-def lib() -> C.CDLL:
-    global _lib
+def lib(fast: bool = False) -> C.CDLL:
+    global _lib, _lib_fast
+    if fast:
+        if _lib_fast is None:
+            if not LIB_FAST.exists():
+                build()
+            _lib_fast = _bind(C.CDLL(str(LIB_FAST)))
+        return _lib_fast
     if _lib is None:
         if not LIB.exists():
             build()
-        L = C.CDLL(str(LIB))
-        sigs = {
-            "oracle_set_threads": (None, [C.c_int]),
-            "oracle_max_threads": (C.c_int, []),
-            "oracle_tables": (None, [_P, _P, _P]),
-            "oracle_feq_f64": (None, [C.c_double] * 4 + [_P]),
-            "oracle_feq_f32": (None, [C.c_float] * 4 + [_P]),
-            "oracle_round_f16": (C.c_float, [C.c_float, C.c_int]),
-            "oracle_classify": (None, [C.c_int, C.c_int, C.c_int, _P, _P, _P]),
-            "oracle_ref_init": (None, [_P, _P, _P, _P, C.c_float, _P, _P, _P, _P]),
-            "oracle_ref_step": (None, [_P, _P, _P, _P, _P, _P, C.c_int]),
-            "oracle_ref_collided": (None, [_P, _P, _P, _P, _P, _P]),
-            "oracle_ext_init_f64": (None, [_P] * 6),
-            "oracle_ext_init_f32": (None, [_P] * 6),
-            "oracle_ext_step_f64": (None, [_P, _P, _P, _P, C.c_int, _P, _P]),
-            "oracle_ext_step_f32": (None, [_P, _P, _P, _P, C.c_int, _P, _P]),
-            "oracle_voxelize_naca": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_float,
-                                               C.c_float, C.c_float, _P]),
-        }
-        for name, (res, args) in sigs.items():
-            fn = getattr(L, name)
-            fn.restype = res
-            fn.argtypes = args
-        _lib = L
+        _lib = _bind(C.CDLL(str(LIB)))
     return _lib
+
+
+def _bind(L: C.CDLL) -> C.CDLL:
+    sigs = {
+        "oracle_set_threads": (None, [C.c_int]),
+        "oracle_max_threads": (C.c_int, []),
+        "oracle_tables": (None, [_P, _P, _P]),
+        "oracle_feq_f64": (None, [C.c_double] * 4 + [_P]),
+        "oracle_feq_f32": (None, [C.c_float] * 4 + [_P]),
+        "oracle_round_f16": (C.c_float, [C.c_float, C.c_int]),
+        "oracle_classify": (None, [C.c_int, C.c_int, C.c_int, _P, _P, _P]),
+        "oracle_ref_init": (None, [_P, _P, _P, _P, C.c_float, _P, _P, _P, _P]),
+        "oracle_ref_step": (None, [_P, _P, _P, _P, _P, _P, C.c_int]),
+        "oracle_ref_collided": (None, [_P, _P, _P, _P, _P, _P]),
+        "oracle_ext_init_f64": (None, [_P] * 6),
+        "oracle_ext_init_f32": (None, [_P] * 6),
+        "oracle_ext_step_f64": (None, [_P, _P, _P, _P, C.c_int, _P, _P]),
+        "oracle_ext_step_f32": (None, [_P, _P, _P, _P, C.c_int, _P, _P]),
+        "oracle_voxelize_naca": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_float,
+                                           C.c_float, C.c_float, _P]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    return L
 
 
 def _p(a) -> int | None:
@@ -62,6 +75,7 @@ def _p(a) -> int | None:
 
 def set_threads(n: int) -> None:
     lib().oracle_set_threads(n)
+    lib(fast=True).oracle_set_threads(n)
 
 
 def max_threads() -> int:
@@ -131,6 +145,14 @@ class RefState:
         lib().oracle_ref_init(_p(self.ip), _p(self.fp), _p(r), _p(uu), rho0, _p(u0a),
                               _p(self.f), _p(self.rho), _p(self.u))
 
+    def set_params(self, tau=None, u_inf=None):
+        """A uniform change between frames (src/main.cpp:1523-1537): the next
+        collide uses the new tau, the next boundary pass the new u_inf."""
+        if tau is not None:
+            self.fp[0] = tau
+        if u_inf is not None:
+            self.fp[1:4] = u_inf
+
     def step(self, n=1):
         lib().oracle_ref_step(_p(self.ip), _p(self.fp), _p(self.mask), _p(self.f), _p(self.rho),
                               _p(self.u), n)
@@ -157,12 +179,26 @@ def _ext_dp(tau, trt_magic, smag_cs, accel, wall, net, open_rho=(0.0, 0.0)):
     return np.ascontiguousarray(np.concatenate(parts), np.float64)
 
 
+def _set_ext_params(dp, tau, accel, wall, smag_cs):
+    if tau is not None:
+        dp[0] = tau
+    if smag_cs is not None:
+        dp[2] = smag_cs
+    if accel is not None:
+        dp[3:6] = accel
+    if wall is not None:
+        dp[6:24] = np.asarray(wall, np.float64).reshape(-1)
+
+
 class ExtState:
     """Textbook stream-collide state: post-collision populations float[19][N]."""
 
     def __init__(self, shape, periodic=(0, 0, 0), tau=0.6, collision=0, trt_magic=3.0 / 16.0,
                  smag_cs=0.0, accel=(0.0, 0.0, 0.0), wall=None, mask=None, dtype=np.float64,
-                 net=None, open_x=(0, 0), open_rho=(0.0, 0.0)):
+                 net=None, open_x=(0, 0), open_rho=(0.0, 0.0), fast=False):
+        """fast: run on the speed build (the timed CPU baseline); results may
+        differ from the checker build in the last place (FMA contraction)."""
+        self.fast = fast
         self.shape = tuple(shape)
         nx, ny, nz = self.shape
         self.n = nx * ny * nz
@@ -178,13 +214,19 @@ class ExtState:
     def init(self, rho, u):
         r = np.ascontiguousarray(np.broadcast_to(rho, (self.n,)), self.dtype)
         uu = np.ascontiguousarray(np.asarray(u, self.dtype).reshape(3, -1) * np.ones((3, self.n)), self.dtype)
-        fn = lib().oracle_ext_init_f64 if self.dtype == np.float64 else lib().oracle_ext_init_f32
+        L = lib(self.fast)
+        fn = L.oracle_ext_init_f64 if self.dtype == np.float64 else L.oracle_ext_init_f32
         fn(_p(self.ip), _p(self.dp), _p(self.mask), _p(r), _p(uu), _p(self.f))
         self.rho[:] = np.where(self.mask == 1, 0, r)
         self.u[:] = np.where(self.mask == 1, 0, uu)
 
+    def set_params(self, tau=None, accel=None, wall=None, smag_cs=None):
+        """New parameters from the next step on (layout of _ext_dp)."""
+        _set_ext_params(self.dp, tau, accel, wall, smag_cs)
+
     def step(self, n=1):
-        fn = lib().oracle_ext_step_f64 if self.dtype == np.float64 else lib().oracle_ext_step_f32
+        L = lib(self.fast)
+        fn = L.oracle_ext_step_f64 if self.dtype == np.float64 else L.oracle_ext_step_f32
         fn(_p(self.ip), _p(self.dp), _p(self.mask), _p(self.f), n, _p(self.rho), _p(self.u))
 
 
@@ -242,6 +284,9 @@ class ExtStateGPU:
         solid = self.mask == 1
         self.rho[solid] = 0
         self.u.view(3, -1)[:, solid] = 0
+
+    def set_params(self, tau=None, accel=None, wall=None, smag_cs=None):
+        _set_ext_params(self.dp, tau, accel, wall, smag_cs)
 
     def step(self, n=1):
         self.torch.cuda.synchronize()

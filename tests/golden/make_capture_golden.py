@@ -1,9 +1,9 @@
 """Regenerates the capture-format fixtures under tests/golden/capture/.
 
-Run in a container where the reference tree is mounted (default
-/root/reference, or $GPU_SIMS_REFERENCE), after building the library:
+Run where the reference tree is available, after building the library, giving its path
+as the argument or in $GPU_SIMS_REFERENCE:
 
-    python tests/golden/make_capture_golden.py
+    python tests/golden/make_capture_golden.py <reference tree>
 
 It writes a small capture (6x4x3 lattice, seeded moments, a mask and a
 full-state population buffer) with this library's host-only writer
@@ -27,7 +27,12 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
-REF = Path(os.environ.get("GPU_SIMS_REFERENCE", "/root/reference"))
+def _reference_root() -> Path:
+    """The reference tree: the first argument, else $GPU_SIMS_REFERENCE."""
+    arg = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GPU_SIMS_REFERENCE")
+    if not arg:
+        raise SystemExit("give the reference tree's path as the argument or in $GPU_SIMS_REFERENCE")
+    return Path(arg)
 OUT = HERE / "capture"
 
 SHAPE = (6, 4, 3)
@@ -49,6 +54,7 @@ def sample_fields():
 
 
 def main() -> int:
+    REF = _reference_root()
     sys.path.insert(0, str(ROOT / "gpu-sims_b200"))
     import types
     import lbm

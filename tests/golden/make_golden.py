@@ -1,9 +1,9 @@
 """Regenerates tests/golden/d3q19_equilibrium.json from the reference.
 
-Run in a container where the reference tree is mounted (default
-/root/reference, or $GPU_SIMS_REFERENCE):
+Run where the reference tree is available, giving its path
+as the argument or in $GPU_SIMS_REFERENCE:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py <reference tree>
 
 It imports the reference's own D3Q19 verifier
 (tools/integrity/integrity/cat3_numerical/d3q19_verify.py), runs its three
@@ -20,11 +20,17 @@ import os
 import sys
 from pathlib import Path
 
-REF = Path(os.environ.get("GPU_SIMS_REFERENCE", "/root/reference"))
+def _reference_root() -> Path:
+    """The reference tree: the first argument, else $GPU_SIMS_REFERENCE."""
+    arg = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GPU_SIMS_REFERENCE")
+    if not arg:
+        raise SystemExit("give the reference tree's path as the argument or in $GPU_SIMS_REFERENCE")
+    return Path(arg)
 OUT = Path(__file__).resolve().parent / "d3q19_equilibrium.json"
 
 
 def main() -> int:
+    REF = _reference_root()
     sys.path.insert(0, str(REF / "tools" / "integrity"))
     from integrity.cat3_numerical import d3q19_verify as v  # noqa: E402
 

@@ -2,10 +2,11 @@
 
 Each test runs the physics-mode step in fp32, fp16-shifted and bf16-shifted
 storage and the FP64 oracle (ExtStep's GPU copy) on the same inputs, and
-checks the errors against written bounds.  The default sizes keep the suite
-short; LBM_FULL_CONFIGS=1 runs the BASELINE sizes (cavity 64^3 x 1000,
-Taylor-Green 384^3 x 2000, channel 512x128x128 x 5000) and, with
-LBM_RESULTS_DIR set, writes each result as JSON there.
+checks the errors against written bounds, at the full workload sizes:
+cavity 64^3 x 1000, Taylor-Green 384^3 x 2000, channel 512x128x128 x 5000,
+and the 256-cavity ensemble x 2000 (fp16 against fp32 storage per domain).
+LBM_QUICK_CONFIGS=1 runs reduced sizes for quick iteration; with
+LBM_RESULTS_DIR set, each result is written as JSON there.
 """
 import json
 import math
@@ -17,7 +18,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-FULL = os.environ.get("LBM_FULL_CONFIGS") == "1"
+FULL = os.environ.get("LBM_QUICK_CONFIGS") != "1"
 LID = 0.05
 
 
@@ -107,7 +108,7 @@ def test_taylor_green_vs_fp64(gpu, oracle):
     from lbm import configs
     N, steps, Nref = (384, 2000, 128) if FULL else (96, 500, 32)
     u0, re = 0.05, 1600.0
-    samples = 20 if FULL else 5
+    samples = 5
     timer = Timer()
     Lc = N / (2 * math.pi)
     tau = 0.5 + 3 * u0 * Lc / re
@@ -196,3 +197,17 @@ def test_channel_vs_fp64(gpu, oracle):
     record("channel", out)
     for name, _ in PRECS:
         assert out[name]["rel_l2_velocity"] <= BOUNDS["channel"][name], (name, out[name]["rel_l2_velocity"])
+
+
+def test_ensemble_f16_vs_f32(gpu):
+    """Config 4: 256 lid-driven cavities (edges from {32..96}, Re in
+    [100, 1000], TRT) advanced together for 2000 steps in fp16-shifted and in
+    fp32 storage; per domain, the relative L2 velocity error of the fp16 run
+    against the fp32 run.  Bounds: median 1e-3, max 1e-2."""
+    from lbm import configs
+    n, steps = (256, 2000) if FULL else (32, 300)
+    out = configs.run_ensemble(steps=steps, n=n, autotune=True)
+    record("ensemble", out)
+    e = out["f16s_vs_f32_rel_l2_velocity"]
+    assert e["median"] <= 1e-3, e
+    assert e["max"] <= 1e-2, e

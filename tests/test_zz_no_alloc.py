@@ -50,3 +50,25 @@ def test_noalloc_rejects_sizes_beyond_its_scratch(gpu):
     assert b"33554432" in lib.lbm_last_error(None)
     assert lib.lbm_conservation_noalloc(None, d_u, 512, out, None) == gpu.ERR_INVALID_ARG
     lat.close()
+
+
+def test_noalloc_at_its_node_limit(gpu):
+    """n = the limit uses every partial slot, and the sums sit right after
+    them.  rho = 1 and a constant u of powers of two make every partial and
+    total exact, so the sums are known: (n, n*ux, n*uy, n*uz)."""
+    import torch
+    lib = gpu.load()
+    torch.cuda.set_device(0)
+    u0 = (0.25, -0.125, 0.0625)
+    d_rho = torch.ones(MAX_NODES, dtype=torch.float32, device="cuda")
+    d_u = torch.empty((3, MAX_NODES), dtype=torch.float32, device="cuda")
+    for a in range(3):
+        d_u[a].fill_(u0[a])
+    torch.cuda.synchronize()
+    out = (C.c_double * 4)()
+    for _ in range(2):
+        rc = lib.lbm_conservation_noalloc(d_rho.data_ptr(), d_u.data_ptr(), MAX_NODES, out, None)
+        assert rc == gpu.OK, lib.lbm_last_error(None).decode()
+        assert list(out) == [float(MAX_NODES)] + [MAX_NODES * v for v in u0]
+    del d_rho, d_u
+    torch.cuda.empty_cache()
