@@ -185,36 +185,50 @@ bool valid_schedule(const lbm_batch_schedule& s) {
          s.test_missing_blocks >= 0;
 }
 
-// Launches nsteps steps (the last one writes the moments).
+// Captures kGraphSteps steps from parity `slot`, without the moment write:
+// kGraphSteps launches of the tile kernel, or in persistent mode one
+// cooperative launch that takes all of them with grid barriers between.
+int build_graph(lbm_batch* b, int slot) {
+  const lbm::BatchLaunch L = launch_of(b);
+  cudaGraph_t g = nullptr;
+  BCK(cudaStreamBeginCapture(b->own, cudaStreamCaptureModeThreadLocal), "begin capture");
+  cudaError_t e = cudaSuccess;
+  if (b->sched.persistent) {
+    e = lbm::batch_persistent(L, lbm_batch::kGraphSteps, slot, b->grid, b->own, false);
+  } else {
+    int P = slot;
+    for (int i = 0; i < lbm_batch::kGraphSteps && e == cudaSuccess; ++i, P ^= 1)
+      e = lbm::batch_step(L, P, false, b->own);
+  }
+  const cudaError_t e2 = cudaStreamEndCapture(b->own, &g);
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return bcuda(b, e != cudaSuccess ? e : e2, "capture batch graph");
+  }
+  e = cudaGraphInstantiate(&b->graph[slot], g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return bcuda(b, e, "instantiate batch graph");
+  return LBM_OK;
+}
+
+// Launches nsteps steps (the last one writes the moments): captured graphs
+// of kGraphSteps steps while more remain (an even count keeps the parity),
+// then the rest directly.
 int run_steps(lbm_batch* b, int nsteps) {
   if (nsteps <= 0) return LBM_OK;
   const lbm::BatchLaunch L = launch_of(b);
-  if (b->sched.persistent) {
-    BCK(lbm::batch_persistent(L, nsteps, b->parity, b->grid, b->stream), "persistent launch");
-    b->parity ^= (nsteps & 1);
-    return LBM_OK;
-  }
   int left = nsteps;
   while (left > lbm_batch::kGraphSteps) {
     const int slot = b->parity;
-    if (!b->graph[slot]) {
-      cudaGraph_t g = nullptr;
-      BCK(cudaStreamBeginCapture(b->own, cudaStreamCaptureModeThreadLocal), "begin capture");
-      cudaError_t e = cudaSuccess;
-      int P = b->parity;
-      for (int i = 0; i < lbm_batch::kGraphSteps && e == cudaSuccess; ++i, P ^= 1)
-        e = lbm::batch_step(L, P, false, b->own);
-      const cudaError_t e2 = cudaStreamEndCapture(b->own, &g);
-      if (e != cudaSuccess || e2 != cudaSuccess) {
-        if (g) cudaGraphDestroy(g);
-        return bcuda(b, e != cudaSuccess ? e : e2, "capture batch graph");
-      }
-      e = cudaGraphInstantiate(&b->graph[slot], g, 0);
-      cudaGraphDestroy(g);
-      if (e != cudaSuccess) return bcuda(b, e, "instantiate batch graph");
-    }
+    if (!b->graph[slot])
+      if (int rc = build_graph(b, slot)) return rc;
     BCK(cudaGraphLaunch(b->graph[slot], b->stream), "batch graph launch");
     left -= lbm_batch::kGraphSteps;
+  }
+  if (b->sched.persistent) {
+    BCK(lbm::batch_persistent(L, left, b->parity, b->grid, b->stream, true), "persistent launch");
+    b->parity ^= (left & 1);
+    return LBM_OK;
   }
   for (int i = 0; i < left; ++i) {
     BCK(lbm::batch_step(L, b->parity, i == left - 1, b->stream), "batch step launch");

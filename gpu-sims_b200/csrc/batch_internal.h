@@ -47,6 +47,9 @@ struct BatchLaunch {
 
 cudaError_t batch_step(const BatchLaunch& L, int P, bool wm, cudaStream_t s);
 cudaError_t batch_persistent_grid(const BatchLaunch& L, int* grid);
-cudaError_t batch_persistent(const BatchLaunch& L, int nsteps, int P0, int grid, cudaStream_t s);
+// One cooperative launch of nsteps steps from parity P0 (after a memset of
+// the barrier state); write_last: its last step writes the moments.
+cudaError_t batch_persistent(const BatchLaunch& L, int nsteps, int P0, int grid, cudaStream_t s,
+                             bool write_last);
 
 }  // namespace lbm

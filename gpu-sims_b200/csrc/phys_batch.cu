@@ -66,6 +66,9 @@ __device__ __forceinline__ void batch_tile(const BatchDomain& D, uint32_t local,
 #ifndef LBM_BATCH_MINB
 #define LBM_BATCH_MINB 4
 #endif
+#ifndef LBM_BATCH_PMINB
+#define LBM_BATCH_PMINB 2
+#endif
 
 template <int PREC, int COLL, bool WM, int P>
 __global__ void __launch_bounds__(256, LBM_BATCH_MINB)
@@ -112,27 +115,40 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned expected, l
   return s_ok != 0;
 }
 
+// write_last: the last step writes the moments (0 for the chunks a CUDA
+// graph replays before the call's final launch).  A launch that finds the
+// timeout bit already set (an earlier barrier gave up; the state needs a new
+// init) returns at once, so replayed chunks after a timeout cost nothing.
 template <int PREC, int COLL>
-__global__ void __launch_bounds__(256, LBM_BATCH_MINB)
+__global__ void __launch_bounds__(256, LBM_BATCH_PMINB)
     k_batch_persistent(const BatchDomain* __restrict__ dp, const uint2* __restrict__ tiles,
                        uint32_t ntiles, int nzt,
-                       int nsteps, int P0, unsigned* bar, unsigned expected, long long spin,
-                       unsigned* status) {
+                       int nsteps, int P0, int write_last, unsigned* bar, unsigned expected,
+                       long long spin, unsigned* status) {
   __shared__ BatchDomain sD;
   __shared__ uint32_t s_local;
-  for (int st = 0; st < nsteps; ++st) {
-    const int P = (P0 + st) & 1;
-    const bool wm = st == nsteps - 1;
+  if (*reinterpret_cast<volatile unsigned*>(status) & BATCH_STATUS_TIMEOUT) return;  // same for every block
+  // one tile loop per (parity, moment write) variant, chosen once per step
+  auto tiles_of_step = [&](auto wm_tag, auto p_tag) {
+    constexpr bool WM = decltype(wm_tag)::value != 0;
+    constexpr int P = decltype(p_tag)::value;
+#pragma unroll 1
     for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
       load_tile(dp, tiles, t, sD, s_local);
-      if (P) {
-        if (wm) batch_tile<PREC, COLL, true, 1>(sD, s_local, nzt, status);
-        else batch_tile<PREC, COLL, false, 1>(sD, s_local, nzt, status);
-      } else {
-        if (wm) batch_tile<PREC, COLL, true, 0>(sD, s_local, nzt, status);
-        else batch_tile<PREC, COLL, false, 0>(sD, s_local, nzt, status);
-      }
+      batch_tile<PREC, COLL, WM, P>(sD, s_local, nzt, status);
       __syncthreads();  // sD is rewritten by the next tile
+    }
+  };
+#pragma unroll 1
+  for (int st = 0; st < nsteps; ++st) {
+    const int P = (P0 + st) & 1;
+    const bool wm = write_last && st == nsteps - 1;
+    if (P) {
+      if (wm) tiles_of_step(IC<1>{}, IC<1>{});
+      else tiles_of_step(IC<0>{}, IC<1>{});
+    } else {
+      if (wm) tiles_of_step(IC<1>{}, IC<0>{});
+      else tiles_of_step(IC<0>{}, IC<0>{});
     }
     if (st + 1 < nsteps && !grid_barrier(bar, expected, spin, status)) return;
   }
@@ -188,7 +204,10 @@ cudaError_t batch_persistent_grid(const BatchLaunch& L, int* grid) {
   return per_sm > 0 ? cudaSuccess : cudaErrorInvalidConfiguration;
 }
 
-cudaError_t batch_persistent(const BatchLaunch& L, int nsteps, int P0, int grid, cudaStream_t s) {
+cudaError_t batch_persistent(const BatchLaunch& L, int nsteps, int P0, int grid, cudaStream_t s,
+                             bool write_last) {
+  // the barrier state is reset by a memset node before every launch, so a
+  // captured launch starts from zero at each replay
   cudaError_t e = cudaMemsetAsync(L.bar, 0, 2 * sizeof(unsigned), s);
   if (e != cudaSuccess) return e;
   const unsigned expected = (unsigned)grid + (unsigned)L.missing_blocks;
@@ -197,11 +216,23 @@ cudaError_t batch_persistent(const BatchLaunch& L, int nsteps, int P0, int grid,
   const uint2* tiles = L.tiles;
   int nzt = L.nzt;
   uint32_t ntiles = L.ntiles;
+  int wl = write_last ? 1 : 0;
   unsigned* bar = L.bar;
   unsigned* status = L.status;
-  void* args[] = {&dom, (void*)&tiles, &ntiles, &nzt, &nsteps, &P0, &bar, (void*)&expected, &spin, &status};
-  return cudaLaunchCooperativeKernel(pick_persistent(L.precision, L.collision), dim3(grid),
-                                     dim3(32, L.rows, 1), args, 0, s);
+  void* args[] = {&dom, (void*)&tiles, &ntiles, &nzt, &nsteps, &P0, &wl, &bar, (void*)&expected, &spin, &status};
+  // a cooperative launch through cudaLaunchKernelExC, which stream capture
+  // records as a cooperative kernel node
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(32, L.rows, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelExC(&cfg, pick_persistent(L.precision, L.collision), args);
 }
 
 }  // namespace lbm

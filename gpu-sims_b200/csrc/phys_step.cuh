@@ -362,60 +362,61 @@ __device__ __forceinline__ bool near_moving(const PhysParams& p, int x_lo, int x
          ((m & (1 << LBM_FACE_ZP)) && !G.per[2] && z == G.nz - 1);
 }
 
-// One fused stream+collide launch.  All lanes of a warp stay converged:
-//  * the 19 slots of the streaming pattern are loaded before the flag byte
-//    is known (a solid node's slots exist, so the loads are in bounds), so a
-//    node costs one memory round trip, not two;
-//  * the five pairs whose forward vector has cx = +1 read and write slot
-//    Y at x+1.  Instead of a 4-byte-shifted warp access, every lane accesses
-//    its own aligned x and the values move one lane by warp shuffle; the
-//    last lane of a warp (or of a row) touches x+1 directly;
-//  * boundary nodes (flag bit) then re-read the bounce-back slots.
-// One warp updates nodes x0 .. x0+31 of row (y, z); y < ny (the caller's
-// test is uniform over the warp).  Used by the single-domain kernel and by
-// the batched kernels (phys_batch.cu).
-//
-// FACE: the open-face variant.  Each lane updates its own node (x0, y, z)
-// with every neighbour slot accessed directly (no shuffles), lane_ok false
-// for idle lanes, and the Zou-He reconstruction before the collision.  The
-// row kernels skip these nodes (FLAG_OPEN); the two sets of nodes read and
-// write disjoint slots, so the face kernel may run after them.
-template <int PREC, int COLL, int SGS, bool FORCE, bool WRITE_MOMENTS, int P, bool FACE = false>
-__device__ __forceinline__ void step_row(const PhysParams& p, const CloNet<SGS>& net,
-                                         void* __restrict__ pop_v,
-                                         const uint8_t* __restrict__ flags,
-                                         const uint32_t* __restrict__ links,
-                                         float* __restrict__ rho_o, float* __restrict__ u_o,
-                                         unsigned* __restrict__ status, const int x0, const int y,
-                                         const int z, const bool lane_ok = true) {
-  using S = Store<PREC>;
-  using T = typename S::T;
+// Index of pair pi among the five pairs with c_x = +1 (pairs 0, 3, 4, 5, 6).
+__host__ __device__ constexpr int xpair_slot(int pi) {
+  int k = 0;
+  for (int q = 0; q < pi; ++q) k += cx(pair_a(q)) > 0 ? 1 : 0;
+  return k;
+}
+static_assert(xpair_slot(8) == 5 && cx(pair_a(6)) > 0 && xpair_slot(6) == 4, "five c_x = +1 pairs");
+
+// A node of step_row between its two phases: the raw stored values of its
+// 19 slots (not yet converted, shuffled or used, so the loads can still be in
+// flight), the raw values an edge lane loads at x+1 for the five c_x = +1
+// pairs, and the node's addressing.
+template <int PREC>
+struct RowNode {
+  using T = typename Store<PREC>::T;
+  T raw[Q];
+  T edge_raw[5];
+  uint8_t fl;
+  bool valid, edge;
+  int x, xc;
+  uint32_t nid, ln;
+  Wrap w;
+};
+
+// Load phase of step_row: the flag byte and every slot of the node's
+// streaming pattern, nothing that consumes a loaded value.  A caller may
+// issue the loads of the next plane before it finishes this one (each slot
+// is read and written by exactly one node per launch, so the two planes'
+// accesses never overlap).
+template <int PREC, int P, bool FACE>
+__device__ __forceinline__ void row_load(const PhysParams& p, bool row_ok, const void* __restrict__ pop_v,
+                                         const uint8_t* __restrict__ flags, const int x0, const int y,
+                                         const int z, const bool lane_ok, RowNode<PREC>& r) {
+  using T = typename Store<PREC>::T;
   const PhysGeom& G = p.g;
   const int lane = threadIdx.x & 31;
-  const int x = FACE ? x0 : x0 + lane;
-  bool row_ok = true;  // y < ny; only the tensor-core closure runs rows beyond
-  if constexpr (SGS == 3) row_ok = net.row_ok;
-  const bool valid = FACE ? lane_ok : x < G.nx && row_ok;
-  const int xc = x < G.nx ? x : G.nx - 1;  // in-bounds address for idle lanes
-  const bool edge = FACE || (lane == 31) || (x >= G.nx - 1);  // touches x+1 itself
-  const uint32_t N = (uint32_t)G.n;
-  const uint32_t nid = (uint32_t)xc + (uint32_t)G.nx * ((uint32_t)y + (uint32_t)G.ny * (uint32_t)z);
-  T* pop = reinterpret_cast<T*>(pop_v);
+  r.x = FACE ? x0 : x0 + lane;
+  r.valid = FACE ? lane_ok : r.x < G.nx && row_ok;
+  r.xc = r.x < G.nx ? r.x : G.nx - 1;  // in-bounds address for idle lanes
+  r.edge = FACE || (lane == 31) || (r.x >= G.nx - 1);  // touches x+1 itself
+  r.nid = (uint32_t)r.xc + (uint32_t)G.nx * ((uint32_t)y + (uint32_t)G.ny * (uint32_t)z);
+  const T* pop = reinterpret_cast<const T*>(pop_v);
   const size_t SS = G.slot_stride;
-  const uint32_t ln = lin32(G, xc, y, z);
-  const Wrap w = wrap_terms(G, xc, y, z);
-
+  r.ln = lin32(G, r.xc, y, z);
+  r.w = wrap_terms(G, r.xc, y, z);
+  const uint32_t ln = r.ln;
+  const Wrap& w = r.w;
   // Faces of non-periodic axes at this node: links across them are half-way
   // bounce-back links known from the coordinates, so their slots are read in
   // the first batch of loads (the y and z parts are uniform over the warp).
-  const bool xlo = !G.per[0] && xc == 0, xhi = !G.per[0] && xc == G.nx - 1;
+  const bool xlo = !G.per[0] && r.xc == 0, xhi = !G.per[0] && r.xc == G.nx - 1;
   const bool ylo = !G.per[1] && y == 0, yhi = !G.per[1] && y == G.ny - 1;
   const bool zlo = !G.per[2] && z == 0, zhi = !G.per[2] && z == G.nz - 1;
-  const bool moving = p.any_moving_wall;
-
-  const uint8_t fl = valid ? flags[nid] : FLAG_SOLID;
-  float g[Q];
-  g[0] = S::raw_ld(pop, ln);
+  r.fl = r.valid ? flags[r.nid] : FLAG_SOLID;
+  r.raw[0] = pop[ln];
   static_for<0, 9>([&](auto PI) {
     constexpr int pi = decltype(PI)::value;
     constexpr int a = pair_a(pi), b = pair_b(pi);
@@ -429,17 +430,74 @@ __device__ __forceinline__ void step_row(const PhysParams& p, const CloNet<SGS>&
     const bool bwd_wall =
         (DX > 0 && xlo) || (DY > 0 && ylo) || (DY < 0 && yhi) || (DZ > 0 && zlo) || (DZ < 0 && zhi);
     // f_a from X = S[1-P](n), or f*_b(n) from S[P](n) across a wall
-    g[a] = S::raw_ld(bwd_wall ? sP : sQ, ln);
-    // f_b from Y = S[P](n+d), or f*_a(n) from S[1-P](n+d) across a wall
+    r.raw[a] = (bwd_wall ? sP : sQ)[ln];
+    // f_b from Y = S[P](n+d), or f*_a(n) from S[1-P](n+d) across a wall; the
+    // c_x = +1 pairs read their own x here (the next lane's value arrives by
+    // shuffle in the second phase) and an edge lane reads x+1 as well
     if (DX == 0) {
-      g[b] = S::raw_ld(fwd_wall ? sQ : sP, ln + offs<0, DY, DZ>(G, w));
+      r.raw[b] = (fwd_wall ? sQ : sP)[ln + offs<0, DY, DZ>(G, w)];
     } else {
-      const float own = S::raw_ld(fyz ? sQ : sP, ln + offs<0, DY, DZ>(G, w));
-      float nb = __shfl_down_sync(FULL, own, 1);
-      if (edge) nb = S::raw_ld(fwd_wall ? sQ : sP, ln + offs<1, DY, DZ>(G, w));
+      constexpr int k = xpair_slot(pi);
+      r.raw[b] = (fyz ? sQ : sP)[ln + offs<0, DY, DZ>(G, w)];
+      if (r.edge) r.edge_raw[k] = (fwd_wall ? sQ : sP)[ln + offs<1, DY, DZ>(G, w)];
+    }
+  });
+}
+
+// The raw values of a deferred load (row_load) in float storage units, with
+// the c_x = +1 pairs' x+1 values shuffled in from the next lane.
+template <int PREC>
+__device__ __forceinline__ void row_convert(const RowNode<PREC>& r, float (&g)[Q]) {
+  using T = typename Store<PREC>::T;
+  auto cvt = [](T v) -> float {
+    if constexpr (PREC == LBM_PREC_F32) return v;
+    else if constexpr (PREC == LBM_PREC_F16S) return __half2float(v);
+    else return __bfloat162float(v);
+  };
+  g[0] = cvt(r.raw[0]);
+  static_for<0, 9>([&](auto PI) {
+    constexpr int pi = decltype(PI)::value;
+    constexpr int a = pair_a(pi), b = pair_b(pi);
+    g[a] = cvt(r.raw[a]);
+    if constexpr (cx(a) == 0) {
+      g[b] = cvt(r.raw[b]);
+    } else {
+      constexpr int k = xpair_slot(pi);
+      float nb = __shfl_down_sync(FULL, cvt(r.raw[b]), 1);
+      if (r.edge) nb = cvt(r.edge_raw[k]);
       g[b] = nb;
     }
   });
+}
+
+// Second phase of a node's step, from its streamed values g (float storage
+// units): the moving-wall and solid-link corrections, the Zou-He faces, the
+// collision, the moments and the stores.  r supplies the addressing (its
+// raw values are not used).
+template <int PREC, int COLL, int SGS, bool FORCE, bool WRITE_MOMENTS, int P, bool FACE>
+__device__ __forceinline__ void row_finish(const PhysParams& p, const CloNet<SGS>& net,
+                                           void* __restrict__ pop_v,
+                                           const uint32_t* __restrict__ links,
+                                           float* __restrict__ rho_o, float* __restrict__ u_o,
+                                           unsigned* __restrict__ status, const int y, const int z,
+                                           const RowNode<PREC>& r, float (&g)[Q]) {
+  using S = Store<PREC>;
+  using T = typename S::T;
+  const PhysGeom& G = p.g;
+  const int lane = threadIdx.x & 31;
+  const int x = r.x, xc = r.xc;
+  const bool valid = r.valid, edge = r.edge;
+  const uint32_t N = (uint32_t)G.n;
+  const uint32_t nid = r.nid, ln = r.ln;
+  const Wrap& w = r.w;
+  const uint8_t fl = r.fl;
+  T* pop = reinterpret_cast<T*>(pop_v);
+  const size_t SS = G.slot_stride;
+  const bool xlo = !G.per[0] && xc == 0, xhi = !G.per[0] && xc == G.nx - 1;
+  const bool ylo = !G.per[1] && y == 0, yhi = !G.per[1] && y == G.ny - 1;
+  const bool zlo = !G.per[2] && z == 0, zhi = !G.per[2] && z == G.nz - 1;
+  const bool moving = p.any_moving_wall;
+
   // Moving-wall momentum terms, in a pass of their own: inside the load loop
   // even a predicated-off add would wait for its load and serialise them.
   if (moving && near_moving(p, xc, xc, y, z)) {
@@ -516,6 +574,90 @@ __device__ __forceinline__ void step_row(const PhysParams& p, const CloNet<SGS>&
       if (fluid && edge) S::raw_st(sP, ln + offs<1, DY, DZ>(G, w), g[a]);
     }
   });
+}
+
+// One fused stream+collide launch.  All lanes of a warp stay converged:
+//  * the 19 slots of the streaming pattern are loaded before the flag byte
+//    is known (a solid node's slots exist, so the loads are in bounds), so a
+//    node costs one memory round trip, not two;
+//  * the five pairs whose forward vector has cx = +1 read and write slot
+//    Y at x+1.  Instead of a 4-byte-shifted warp access, every lane accesses
+//    its own aligned x and the values move one lane by warp shuffle; the
+//    last lane of a warp (or of a row) touches x+1 directly;
+//  * boundary nodes (flag bit) then re-read the bounce-back slots.
+// One warp updates nodes x0 .. x0+31 of row (y, z); y < ny (the caller's
+// test is uniform over the warp).  Used by the single-domain kernel and by
+// the batched kernels (phys_batch.cu).
+//
+// FACE: the open-face variant.  Each lane updates its own node (x0, y, z)
+// with every neighbour slot accessed directly (no shuffles), lane_ok false
+// for idle lanes, and the Zou-He reconstruction before the collision.  The
+// row kernels skip these nodes (FLAG_OPEN); the two sets of nodes read and
+// write disjoint slots, so the face kernel may run after them.
+template <int PREC, int COLL, int SGS, bool FORCE, bool WRITE_MOMENTS, int P, bool FACE = false>
+__device__ __forceinline__ void step_row(const PhysParams& p, const CloNet<SGS>& net,
+                                         void* __restrict__ pop_v,
+                                         const uint8_t* __restrict__ flags,
+                                         const uint32_t* __restrict__ links,
+                                         float* __restrict__ rho_o, float* __restrict__ u_o,
+                                         unsigned* __restrict__ status, const int x0, const int y,
+                                         const int z, const bool lane_ok = true) {
+  using S = Store<PREC>;
+  using T = typename S::T;
+  const PhysGeom& G = p.g;
+  const int lane = threadIdx.x & 31;
+  bool row_ok = true;  // y < ny; only the tensor-core closure runs rows beyond
+  if constexpr (SGS == 3) row_ok = net.row_ok;
+  RowNode<PREC> r;
+  r.x = FACE ? x0 : x0 + lane;
+  r.valid = FACE ? lane_ok : r.x < G.nx && row_ok;
+  r.xc = r.x < G.nx ? r.x : G.nx - 1;  // in-bounds address for idle lanes
+  r.edge = FACE || (lane == 31) || (r.x >= G.nx - 1);  // touches x+1 itself
+  r.nid = (uint32_t)r.xc + (uint32_t)G.nx * ((uint32_t)y + (uint32_t)G.ny * (uint32_t)z);
+  T* pop = reinterpret_cast<T*>(pop_v);
+  const size_t SS = G.slot_stride;
+  r.ln = lin32(G, r.xc, y, z);
+  r.w = wrap_terms(G, r.xc, y, z);
+  const uint32_t ln = r.ln;
+  const Wrap& w = r.w;
+  const bool edge = r.edge;
+
+  // Faces of non-periodic axes at this node: links across them are half-way
+  // bounce-back links known from the coordinates, so their slots are read in
+  // the first batch of loads (the y and z parts are uniform over the warp).
+  const bool xlo = !G.per[0] && r.xc == 0, xhi = !G.per[0] && r.xc == G.nx - 1;
+  const bool ylo = !G.per[1] && y == 0, yhi = !G.per[1] && y == G.ny - 1;
+  const bool zlo = !G.per[2] && z == 0, zhi = !G.per[2] && z == G.nz - 1;
+
+  r.fl = r.valid ? flags[r.nid] : FLAG_SOLID;
+  float g[Q];
+  g[0] = S::raw_ld(pop, ln);
+  static_for<0, 9>([&](auto PI) {
+    constexpr int pi = decltype(PI)::value;
+    constexpr int a = pair_a(pi), b = pair_b(pi);
+    constexpr int DX = cx(a), DY = cy(a), DZ = cz(a);
+    const T* s0 = pop + (size_t)(1 + 2 * pi) * SS;
+    const T* sP = P ? s0 + SS : s0;
+    const T* sQ = P ? s0 : s0 + SS;
+    // n + d (forward) or n - d (backward) beyond a wall face
+    const bool fyz = (DY > 0 && yhi) || (DY < 0 && ylo) || (DZ > 0 && zhi) || (DZ < 0 && zlo);
+    const bool fwd_wall = fyz || (DX > 0 && xhi);
+    const bool bwd_wall =
+        (DX > 0 && xlo) || (DY > 0 && ylo) || (DY < 0 && yhi) || (DZ > 0 && zlo) || (DZ < 0 && zhi);
+    // f_a from X = S[1-P](n), or f*_b(n) from S[P](n) across a wall
+    g[a] = S::raw_ld(bwd_wall ? sP : sQ, ln);
+    // f_b from Y = S[P](n+d), or f*_a(n) from S[1-P](n+d) across a wall
+    if (DX == 0) {
+      g[b] = S::raw_ld(fwd_wall ? sQ : sP, ln + offs<0, DY, DZ>(G, w));
+    } else {
+      const float own = S::raw_ld(fyz ? sQ : sP, ln + offs<0, DY, DZ>(G, w));
+      float nb = __shfl_down_sync(FULL, own, 1);
+      if (edge) nb = S::raw_ld(fwd_wall ? sQ : sP, ln + offs<1, DY, DZ>(G, w));
+      g[b] = nb;
+    }
+  });
+  row_finish<PREC, COLL, SGS, FORCE, WRITE_MOMENTS, P, FACE>(p, net, pop_v, links, rho_o, u_o, status, y,
+                                                             z, r, g);
 }
 
 // Two nodes per thread (step_row2) need an even row length, so that pairs

@@ -163,10 +163,22 @@ __global__ void __launch_bounds__(STEP_THREADS, LBM_TC_MINB)
   c.row_ok = y < p.g.ny;
   const int z0 = blockIdx.z * LBM_TC_ZPB;
   const int z1 = min(p.g.nz, z0 + LBM_TC_ZPB);  // uniform over the CTA
+  const int yr = c.row_ok ? y : p.g.ny - 1;
+  const int x0 = blockIdx.x * 32;
+  // Software pipeline over the planes: the loads of plane z+1 are issued
+  // before plane z's collision, whose MMA wait and arithmetic then hide their
+  // latency (each slot belongs to one node, so the two planes never touch
+  // the same slot).
+  RowNode<PREC> cur, nxt;
+  row_load<PREC, P, false>(p, c.row_ok, pop_v, flags, x0, yr, z0, true, cur);
   for (int z = z0; z < z1; ++z) {
     c.phase = (uint32_t)((z - z0) & 1);
-    step_row<PREC, COLL, 3, false, WRITE_MOMENTS, P>(p, c, pop_v, flags, links, rho_o, u_o, status,
-                                                     blockIdx.x * 32, c.row_ok ? y : p.g.ny - 1, z);
+    float g[Q];
+    row_convert(cur, g);  // waits for plane z's loads
+    if (z + 1 < z1) row_load<PREC, P, false>(p, c.row_ok, pop_v, flags, x0, yr, z + 1, true, nxt);
+    row_finish<PREC, COLL, 3, false, WRITE_MOMENTS, P, false>(p, c, pop_v, links, rho_o, u_o, status, yr, z,
+                                                              cur, g);
+    cur = nxt;
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   const bool aborted = __syncthreads_or(gave_up[threadIdx.y] != 0);

@@ -103,6 +103,39 @@ def test_persistent_barrier_timeout_is_reported(gpu):
     b.close()
 
 
+def test_persistent_graph_replays_after_a_timeout(gpu):
+    """Persistent launches replayed from a captured graph (a call of more than
+    16 steps): the first launch's barrier runs out, the replays after it find
+    the timeout bit and return at once, and the call reports LBM_ERR_TIMEOUT
+    in about the time of one bounded wait."""
+    import time
+    descs = domain_descs(gpu)
+    b = batch_of(gpu, descs)
+    b.set_schedule(persistent=1, spin_limit_cycles=2_000_000, test_missing_blocks=1)
+    t0 = time.perf_counter()
+    b.step(70)  # 4 graph replays of 16 steps, then 6 steps launched directly
+    with pytest.raises(gpu.LbmError) as e:
+        b.sync()
+    assert e.value.code == gpu.ERR_TIMEOUT
+    assert time.perf_counter() - t0 < 5.0
+    b.close()
+
+
+def test_persistent_graph_many_steps(gpu):
+    """A long call in persistent mode (graph replays of one cooperative launch
+    of 16 steps each, then the rest) equals the single-domain runs."""
+    descs = domain_descs(gpu, 1, 1)
+    steps = 16 * 5 + 3
+    want = singles(gpu, descs, steps)
+    b = batch_of(gpu, descs)
+    b.set_schedule(rows_per_block=4, z_per_thread=4, persistent=1)
+    b.step(steps)
+    b.sync()
+    for i in range(len(descs)):
+        assert np.array_equal(b.read_populations(i), want[i][0]), i
+    b.close()
+
+
 def test_autotune_restores_state(gpu):
     descs = domain_descs(gpu, 1, 0)
     b = batch_of(gpu, descs)
