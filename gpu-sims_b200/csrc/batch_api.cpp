@@ -208,6 +208,7 @@ int build_graph(lbm_batch* b, int slot) {
   e = cudaGraphInstantiate(&b->graph[slot], g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return bcuda(b, e, "instantiate batch graph");
+  BCK(cudaGraphUpload(b->graph[slot], b->stream), "upload batch graph");
   return LBM_OK;
 }
 

@@ -436,6 +436,9 @@ static int build_graph(lbm_ctx* c, int slot) {
   e = cudaGraphInstantiate(&c->graph[slot], g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return cuda_fail(c, e, "instantiate step graph");
+  // upload now, so that its first launch does not pay for it inside a
+  // caller's step loop
+  CK(cudaGraphUpload(c->graph[slot], c->stream), "upload step graph");
   return LBM_OK;
 }
 

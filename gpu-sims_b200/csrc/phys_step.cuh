@@ -844,11 +844,10 @@ __device__ __forceinline__ void step_row2(const PhysParams& p, const CloNet<SGS>
 
   const bool both = fluidA && fluidB;
   const bool passB = fluidB && !edge;  // node B's Y value at x+2 is stored by lane+1
-  // The store phase.  fp32 compiles it twice: FAST for warps whose every pair
-  // stores both nodes (a warp-uniform vote), with plain vector stores, and the
-  // general form for the rest (measured on B200, channel 512x128x128: 37.4
-  // GLUPS against 36.2).  The 2-byte formats ran 1 % slower that way and keep
-  // the general form only.
+  // The store phase is compiled twice: FAST for warps whose every pair stores
+  // both nodes (a warp-uniform vote), with plain vector stores, and the
+  // general form for the rest (measured on B200, channel 512x128x128: fp32
+  // 37.4 GLUPS against 36.2; fp16 with one-warp blocks 53.7 against 52.0).
   auto stores = [&](auto fast_tag) {
     constexpr bool FAST = decltype(fast_tag)::value != 0;
     // store node A / node B values at slot positions i (A) and i+1 (B)
@@ -883,7 +882,10 @@ __device__ __forceinline__ void step_row2(const PhysParams& p, const CloNet<SGS>
       }
     });
   };
-  if constexpr (PREC == LBM_PREC_F32) {
+#ifndef LBM_VOTE_STORES16
+#define LBM_VOTE_STORES16 1
+#endif
+  if constexpr (PREC == LBM_PREC_F32 || LBM_VOTE_STORES16) {
     if (__all_sync(FULL, both)) stores(IC<1>{});
     else stores(IC<0>{});
   } else {

@@ -13,7 +13,7 @@ namespace {
 // the 2-byte formats are issue-bound rather than memory-bound: their
 // residency bound is tuned separately
 #ifndef LBM_STEP2_MINB16
-#define LBM_STEP2_MINB16 5
+#define LBM_STEP2_MINB16 6
 #endif
 // Residency bounds of the learned-closure kernels (the MLP's hidden layer
 // stays in registers: two nodes' worth in the pair kernel).
@@ -24,16 +24,20 @@ namespace {
 #define LBM_CLO2_MINB 2
 #endif
 
-// Rows per block of the pair kernel.  fp32 runs one-warp blocks whose row is
+// Rows per block of the pair kernel.  One-warp blocks whose row is
 // blockIdx.y: y is then warp-uniform to the compiler, which moves the row's
 // wall predicates, wrap terms and slot selection to the uniform datapath
-// (measured on B200, channel 512x128x128: 36.55 GLUPS against 35.74 with
-// four-row blocks).  The 2-byte formats keep four-row blocks: with one-warp
-// blocks their register cap of 96 (five warps per scheduler) spilled and they
-// ran slower (42.8 GLUPS against 51.1; 47.4 with 16 blocks per SM).
+// (measured on B200, channel 512x128x128: fp32 36.55 GLUPS against 35.74 with
+// four-row blocks; fp16 52.0 against 51.1, and 53.7 with the vote-based store
+// phase of step_row2, which alone on four-row blocks ran 50.2).  The 2-byte
+// kernel fits its 102-register bound (20 one-warp blocks per SM) without
+// spills; an earlier form of it spilled there.
+#ifndef LBM_STEP2_ROWS16
+#define LBM_STEP2_ROWS16 1
+#endif
 template <int PREC, int SGS>
 constexpr int step2_rows() {
-  return (PREC == LBM_PREC_F32 && SGS != 2) ? 1 : STEP_BY;
+  return SGS == 2 ? STEP_BY : (PREC == LBM_PREC_F32 ? 1 : LBM_STEP2_ROWS16);
 }
 
 // Two nodes per thread (step_pairs(nx)): a warp covers 64 consecutive x.
@@ -42,7 +46,8 @@ template <int PREC, int COLL, int SGS, bool FORCE, bool WRITE_MOMENTS, int P>
 __global__ void __launch_bounds__(32 * step2_rows<PREC, SGS>(),
                                   SGS == 2 ? LBM_CLO2_MINB
                                            : (PREC == LBM_PREC_F32 ? LBM_STEP2_MINB * STEP_BY
-                                                                   : LBM_STEP2_MINB16))
+                                                                   : LBM_STEP2_MINB16 * STEP_BY /
+                                                                         LBM_STEP2_ROWS16))
     k_phys_step2(PhysParams p, void* __restrict__ pop_v, const uint8_t* __restrict__ flags,
                  const uint32_t* __restrict__ links, float* __restrict__ rho_o,
                  float* __restrict__ u_o, unsigned* __restrict__ status,

@@ -319,6 +319,28 @@ def test_network_beats_constant_a_priori(gpu):
     assert l_net < 0.97 * l_const and l_const <= l_smag, (l_net, l_const, l_smag)
 
 
+def test_network_beats_smagorinsky_a_posteriori(gpu):
+    """What the trained network gains in the coarse simulation itself.  The
+    experiment of lbm.closure.run at reduced size: fine 256^3 periodic HIT
+    (tau 0.508, 8000 steps), filtered x4 to 64^3; the network is trained on
+    seed 5 and one scale of its Cs^2 is calibrated on that run's own filtered
+    spectra; the evaluation is a held-out fine run (seed 6).  From that run's
+    filtered initial field, the coarse run with the learned closure must
+    track the filtered fine spectra (relative error, 1 <= k <= 12, averaged
+    over the samples every 125 coarse steps) better than plain Smagorinsky
+    at Cs = 0.1 (measured: 15.4 % against 30.0 %)."""
+    import torch
+    from lbm import closure as cl
+    res = cl.run(fine=256, factor=4, tau_f=0.508, snapshots=1000, every=8, samples_per_snapshot=4096,
+                 eval_every=125, kmax=12, calibrate=(0.25, 0.35, 0.5, 0.75, 1.0), verbose=False)
+    torch.cuda.set_stream(torch.cuda.default_stream())
+    learned, smag = res["learned"], res["smagorinsky"]
+    assert learned["finite"] and smag["finite"]
+    assert learned["time_mean"] < 0.8 * smag["time_mean"], (learned["time_mean"], smag["time_mean"])
+    # the coarse run is cheaper than the fine run it stands in for
+    assert learned["wall_ratio"] > 20.0, learned["wall_ratio"]
+
+
 @pytest.mark.parametrize("shape", [(32, 12, 10), (40, 9, 6)])
 def test_tensor_core_mlp_matches_cuda_core_mlp(gpu, oracle, shape):
     """Variant 8 evaluates the hidden layer with tcgen05 MMAs (bf16
