@@ -59,13 +59,24 @@ __global__ void __launch_bounds__(32 * step2_rows<PREC, SGS>(),
                                                       status, blockIdx.x * 64, y, blockIdx.z);
 }
 
+// Rows per block of the one-node kernel (1: one-warp blocks, row = blockIdx.y).
+#ifndef LBM_STEP1_ROWS
+#define LBM_STEP1_ROWS STEP_BY
+#endif
+template <int SGS>
+constexpr int step1_rows() {
+  return SGS == 2 ? STEP_BY : LBM_STEP1_ROWS;
+}
+
 template <int PREC, int COLL, int SGS, bool FORCE, bool WRITE_MOMENTS, int P>
-__global__ void __launch_bounds__(STEP_THREADS, SGS == 2 ? LBM_CLO_MINB : LBM_STEP_MINB)
+__global__ void __launch_bounds__(32 * step1_rows<SGS>(),
+                                  SGS == 2 ? LBM_CLO_MINB : LBM_STEP_MINB * STEP_BY / step1_rows<SGS>())
     k_phys_step(PhysParams p, void* __restrict__ pop_v, const uint8_t* __restrict__ flags,
                 const uint32_t* __restrict__ links, float* __restrict__ rho_o,
                 float* __restrict__ u_o, unsigned* __restrict__ status,
                 const __grid_constant__ CloNet<SGS> net) {
-  const int y = blockIdx.y * STEP_BY + threadIdx.y;
+  constexpr int R = step1_rows<SGS>();
+  const int y = R == 1 ? (int)blockIdx.y : (int)(blockIdx.y * R + threadIdx.y);
   if (y >= p.g.ny) return;  // uniform over the warp
   step_row<PREC, COLL, SGS, FORCE, WRITE_MOMENTS, P>(p, net, pop_v, flags, links, rho_o, u_o,
                                                      status, blockIdx.x * 32, y, blockIdx.z);
@@ -259,9 +270,10 @@ cudaError_t launch_rows(const Ctx& c, int P, bool wm, cudaStream_t s) {
 #undef LBM_STEP_LAUNCH
     return cudaGetLastError();
   }
-  const dim3 grd((G.nx + 31) / 32, (G.ny + STEP_BY - 1) / STEP_BY, G.nz);
+  constexpr int R1 = step1_rows<SGS>();
+  const dim3 grd((G.nx + 31) / 32, (G.ny + R1 - 1) / R1, G.nz), blk1(32, R1, 1);
 #define LBM_STEP_LAUNCH(WM, PAR)                                          \
-  k_phys_step<PREC, COLL, SGS, FORCE, WM, PAR><<<grd, blk, 0, s>>>(       \
+  k_phys_step<PREC, COLL, SGS, FORCE, WM, PAR><<<grd, blk1, 0, s>>>(      \
       c.pp, c.pop, c.flags, c.links, c.rho, c.u, c.status, net)
   if (wm) {
     if (P) LBM_STEP_LAUNCH(true, 1); else LBM_STEP_LAUNCH(true, 0);
