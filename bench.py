@@ -311,7 +311,9 @@ def run_ours(args, world, rank, local):
         pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
         m_h, r_h, u_h = pin(mask), pin(rho), pin(u)
         r_out = torch.empty(n, dtype=torch.float32).pin_memory().numpy()
-        u_out = torch.empty((n, 3), dtype=torch.float32).pin_memory().numpy()
+        # the velocity as the reference's consumers read it back: rgba16f
+        # (capture_save and the VDB export, src/main.cpp:1290-1296, 1771-1779)
+        u_out = torch.empty((n, 4), dtype=torch.int16).pin_memory().numpy().view(np.uint16)
         d = lbm.default_desc(nx=SHAPE[0], ny=SHAPE[1], nz=SHAPE[2], mode=lbm.MODE_PHYSICS,
                              precision=precision, collision=lbm.COLL_BGK, periodic=(1, 0, 0),
                              tau=TAU, body_accel=ACCEL)
@@ -335,7 +337,7 @@ def run_ours(args, world, rank, local):
                     sums[i] = lat.conservation()
                 else:
                     lat.conservation_async(sums[i].ctypes.data)
-            rc = lib.lbm_read_moments(lat._h, r_out.ctypes.data, u_out.ctypes.data, lbm.U_F32X3)
+            rc = lib.lbm_read_moments(lat._h, r_out.ctypes.data, u_out.ctypes.data, lbm.U_F16X4)
             assert rc == 0
             torch.cuda.synchronize()
             return ranks_max(time.perf_counter() - t0)
@@ -352,8 +354,9 @@ def run_ours(args, world, rank, local):
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "what": "flags + initial moments uploaded from pinned host memory, per step one "
                         "lbm_step(1) and a read of that step's fp64 conservation sums into pinned "
-                        "host memory (lbm_conservation_async: no host wait per step), final rho/u "
-                        "read to pinned host memory",
+                        "host memory (lbm_conservation_async: no host wait per step), final rho (f32) "
+                        "and u (rgba16f, as the reference's capture and VDB export read it) to pinned "
+                        "host memory",
                 "blocking": {"value": aggregate_mlups(n, args.steps, dt_block, world), "unit": "MLUPS",
                              "what": "the same with lbm_conservation (a host wait every step)"}}
 
