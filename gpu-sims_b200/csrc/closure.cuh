@@ -53,6 +53,7 @@ template <> struct CloNet<3> {
   const CloNet<2>* net;     // parameters (kernel parameter space)
   uint8_t* sA;              // two A tiles: 128 rows x 32 bf16 each, canonical K-major layout
   uint32_t sA_addr, sB_addr, mbar_addr;  // shared-window addresses
+  uint32_t sB1_addr;        // W1 tile (first layer on the tensor cores)
   uint32_t tmem;            // TMEM base (lane 0, first column)
   unsigned* status;
   uint32_t* gave_up;        // shared, one word per warp: that warp's wait ran out
@@ -62,6 +63,12 @@ template <> struct CloNet<3> {
   __device__ __forceinline__ float operator[](int k) const { return net->v[k]; }
 };
 constexpr int CLO_TILE_A_BYTES = 128 * 64;
+// First layer (9 -> 32) on the tensor cores as well: one K = 16 MMA of the
+// bf16 standardised features (zero-padded) against W1, before the 32 x 32
+// layer.  0: the first layer on the CUDA cores in fp32.
+#ifndef LBM_TC_LAYER1
+#define LBM_TC_LAYER1 1
+#endif
 
 // Shared-memory matrix descriptor of a K-major tile without swizzle: 8-row x
 // 16-byte core matrices, rows 16 B apart, K-adjacent core matrices `lbo`
@@ -144,73 +151,20 @@ __device__ __forceinline__ typename O::F closure_mlp(const W& w, const typename 
 
 // The tensor-core evaluation of CloNet<3> (see there); every thread of the
 // CTA calls it once, with its own node's raw inputs.
-__device__ __forceinline__ float closure_mlp_tc(const CloNet<3>& c, const float (&xr)[CLO_IN]) {
-  const CloNet<2>& w = *c.net;
-  const int r = threadIdx.y * 32 + threadIdx.x;
-  float x[CLO_IN];
-#pragma unroll
-  for (int j = 0; j < CLO_IN; ++j) x[j] = __fmul_rn(__fsub_rn(xr[j], w.v[CLO_MEAN + j]), w.v[CLO_ISCALE + j]);
-  uint32_t hp[CLO_HID / 2];
-#pragma unroll
-  for (int i = 0; i < CLO_HID; i += 2) {
-    float a0 = w.v[CLO_B1 + i], a1 = w.v[CLO_B1 + i + 1];
-#pragma unroll
-    for (int j = 0; j < CLO_IN; ++j) {
-      a0 = __fmaf_rn(w.v[CLO_W1 + i * CLO_IN + j], x[j], a0);
-      a1 = __fmaf_rn(w.v[CLO_W1 + (i + 1) * CLO_IN + j], x[j], a1);
-    }
-    const __nv_bfloat162 h = __floats2bfloat162_rn(fmaxf(a0, 0.f), fmaxf(a1, 0.f));
-    hp[i / 2] = *reinterpret_cast<const uint32_t*>(&h);
-  }
-  // this warp's own mark (only it writes it): the same value in every lane
-  const bool warp_gave_up = c.gave_up[threadIdx.y] != 0;
-  const uint32_t buf = c.phase * CLO_TILE_A_BYTES;
-  uint8_t* row = c.sA + buf + clo_tile_off(r, 0);
-  if (!warp_gave_up) {
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-      *reinterpret_cast<uint4*>(row + q * 128) =
-          make_uint4(hp[4 * q], hp[4 * q + 1], hp[4 * q + 2], hp[4 * q + 3]);
-  }
-  // the A tile is visible to the tensor core, and every thread has finished
-  // reading the previous evaluation's D, before the MMAs are issued
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  const bool abort = __syncthreads_or(warp_gave_up);  // uniform over the CTA
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (abort) return 1.0f;  // a wait ran out earlier in this launch: no more MMAs
-  if (r == 0) {
-    *c.last_phase = c.phase;
-#pragma unroll
-    for (int kk = 0; kk < 2; ++kk) {
-      const uint64_t da = clo_smem_desc(c.sA_addr + buf + kk * 256, 128, 512);
-      const uint64_t db = clo_smem_desc(c.sB_addr + kk * 256, 128, 512);
-      asm volatile(
-          "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-          "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
-          :: "r"(c.tmem), "l"(da), "l"(db), "r"(CLO_IDESC), "r"(kk) : "memory");
-    }
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                 :: "r"(c.mbar_addr) : "memory");
-  }
+// Bounded wait for the mbarrier phase of the given parity: true when it
+// completed, per warp (the tensor-memory load after it is warp-collective).
+__device__ __forceinline__ bool clo_wait(const CloNet<3>& c, uint32_t parity) {
   uint32_t done = 0;
   for (int it = 0; it < LBM_CLO_WAIT_LIMIT && !done; ++it)
     asm volatile(
         "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
         "selp.b32 %0, 1, 0, P1;\n\t}\n"
-        : "=r"(done) : "r"(c.mbar_addr), "r"(c.phase) : "memory");
-  // the tensor-memory load below is warp-collective: decide per warp
-  if (!__all_sync(0xffffffffu, done != 0)) {  // gave up: plain Smagorinsky, error reported at sync
-    if (threadIdx.x == 0) {
-      c.gave_up[threadIdx.y] = 1u;
-      atomicOr(c.status, 2u);
-    }
-    __syncwarp();
-    return 1.0f;
-  }
-  __syncwarp();
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  uint32_t v[CLO_HID];
+        : "=r"(done) : "r"(c.mbar_addr), "r"(parity) : "memory");
+  return __all_sync(0xffffffffu, done != 0);
+}
+
+// The warp's 32 accumulator columns (its 32 TMEM lanes) into registers.
+__device__ __forceinline__ void clo_tmem_ld(const CloNet<3>& c, uint32_t (&v)[CLO_HID]) {
   const uint32_t ta = c.tmem + ((uint32_t)(threadIdx.y * 32) << 16);
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
@@ -222,6 +176,139 @@ __device__ __forceinline__ float closure_mlp_tc(const CloNet<3>& c, const float 
         "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
       : "r"(ta));
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// One MMA of K = 16 (kk: which K half of the 32-column tiles) into the
+// accumulator; accumulate = 0 overwrites it.
+__device__ __forceinline__ void clo_mma(const CloNet<3>& c, uint32_t a_addr, uint32_t b_addr, int accumulate) {
+  const uint64_t da = clo_smem_desc(a_addr, 128, 512);
+  const uint64_t db = clo_smem_desc(b_addr, 128, 512);
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+      :: "r"(c.tmem), "l"(da), "l"(db), "r"(CLO_IDESC), "r"(accumulate) : "memory");
+}
+
+__device__ __forceinline__ void clo_commit(const CloNet<3>& c, uint32_t parity) {
+  *c.last_phase = parity;
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+               :: "r"(c.mbar_addr) : "memory");
+}
+
+// The A tile is visible to the tensor core and every thread has finished its
+// tensor-memory loads; true (uniform) when any warp has given up a wait in
+// this launch, in which case every warp marks itself so that none writes an
+// A tile again.
+__device__ __forceinline__ bool clo_barrier_abort(const CloNet<3>& c, bool warp_gave_up) {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  const bool abort = __syncthreads_or(warp_gave_up);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (abort && threadIdx.x == 0) c.gave_up[threadIdx.y] = 1u;
+  __syncwarp();
+  return abort;
+}
+
+__device__ __forceinline__ void clo_give_up(const CloNet<3>& c) {
+  if (threadIdx.x == 0) {
+    c.gave_up[threadIdx.y] = 1u;
+    atomicOr(c.status, 2u);
+  }
+  __syncwarp();
+}
+
+// The tensor-core evaluation of CloNet<3> (see there); every thread of the
+// CTA calls it once, with its own node's raw inputs.  With LBM_TC_LAYER1 the
+// mbarrier completes twice per evaluation (parities 0 and 1), else once (the
+// evaluation's parity).
+__device__ __forceinline__ float closure_mlp_tc(const CloNet<3>& c, const float (&xr)[CLO_IN]) {
+  const CloNet<2>& w = *c.net;
+  const int r = threadIdx.y * 32 + threadIdx.x;
+  float x[CLO_IN];
+#pragma unroll
+  for (int j = 0; j < CLO_IN; ++j) x[j] = __fmul_rn(__fsub_rn(xr[j], w.v[CLO_MEAN + j]), w.v[CLO_ISCALE + j]);
+  // this warp's own mark (only it writes it): the same value in every lane
+  const bool warp_gave_up = c.gave_up[threadIdx.y] != 0;
+  const uint32_t buf = c.phase * CLO_TILE_A_BYTES;
+  uint8_t* row = c.sA + buf + clo_tile_off(r, 0);
+  uint32_t hp[CLO_HID / 2];
+  uint32_t parity2 = c.phase;  // parity of the hidden layer's commit
+  if constexpr (LBM_TC_LAYER1) {
+    // A = the features in bf16, k < 9, zeros to k = 16
+    uint32_t xp[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const float lo = 2 * q < CLO_IN ? x[2 * q] : 0.f, hi = 2 * q + 1 < CLO_IN ? x[2 * q + 1] : 0.f;
+      const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+      xp[q] = *reinterpret_cast<const uint32_t*>(&h);
+    }
+    if (!warp_gave_up) {
+      *reinterpret_cast<uint4*>(row) = make_uint4(xp[0], xp[1], xp[2], xp[3]);
+      *reinterpret_cast<uint4*>(row + 128) = make_uint4(xp[4], xp[5], xp[6], xp[7]);
+    }
+    if (clo_barrier_abort(c, warp_gave_up)) return 1.0f;
+    if (r == 0) {
+      clo_mma(c, c.sA_addr + buf, c.sB1_addr, 0);
+      clo_commit(c, 0u);
+    }
+    bool mine = !warp_gave_up;
+    if (!clo_wait(c, 0u)) {  // gave up: r = 1 after the next barrier
+      clo_give_up(c);
+      mine = false;
+    }
+    if (mine) {
+      __syncwarp();
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      uint32_t d[CLO_HID];
+      clo_tmem_ld(c, d);
+#pragma unroll
+      for (int i = 0; i < CLO_HID; i += 2) {
+        const float a0 = __fadd_rn(__uint_as_float(d[i]), w.v[CLO_B1 + i]);
+        const float a1 = __fadd_rn(__uint_as_float(d[i + 1]), w.v[CLO_B1 + i + 1]);
+        const __nv_bfloat162 h = __floats2bfloat162_rn(fmaxf(a0, 0.f), fmaxf(a1, 0.f));
+        hp[i / 2] = *reinterpret_cast<const uint32_t*>(&h);
+      }
+      // the first MMA has completed: its A tile may be overwritten
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        *reinterpret_cast<uint4*>(row + q * 128) =
+            make_uint4(hp[4 * q], hp[4 * q + 1], hp[4 * q + 2], hp[4 * q + 3]);
+    }
+    parity2 = 1u;
+    if (clo_barrier_abort(c, c.gave_up[threadIdx.y] != 0)) return 1.0f;
+  } else {
+#pragma unroll
+    for (int i = 0; i < CLO_HID; i += 2) {
+      float a0 = w.v[CLO_B1 + i], a1 = w.v[CLO_B1 + i + 1];
+#pragma unroll
+      for (int j = 0; j < CLO_IN; ++j) {
+        a0 = __fmaf_rn(w.v[CLO_W1 + i * CLO_IN + j], x[j], a0);
+        a1 = __fmaf_rn(w.v[CLO_W1 + (i + 1) * CLO_IN + j], x[j], a1);
+      }
+      const __nv_bfloat162 h = __floats2bfloat162_rn(fmaxf(a0, 0.f), fmaxf(a1, 0.f));
+      hp[i / 2] = *reinterpret_cast<const uint32_t*>(&h);
+    }
+    if (!warp_gave_up) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        *reinterpret_cast<uint4*>(row + q * 128) =
+            make_uint4(hp[4 * q], hp[4 * q + 1], hp[4 * q + 2], hp[4 * q + 3]);
+    }
+    if (clo_barrier_abort(c, warp_gave_up)) return 1.0f;  // no more MMAs
+  }
+  if (r == 0) {
+#pragma unroll
+    for (int kk = 0; kk < 2; ++kk) clo_mma(c, c.sA_addr + buf + kk * 256, c.sB_addr + kk * 256, kk);
+    clo_commit(c, parity2);
+  }
+  if (!clo_wait(c, parity2)) {  // gave up: plain Smagorinsky, error reported at sync
+    clo_give_up(c);
+    return 1.0f;
+  }
+  __syncwarp();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  uint32_t v[CLO_HID];
+  clo_tmem_ld(c, v);
   float z = w.v[CLO_B3];
 #pragma unroll
   for (int i = 0; i < CLO_HID; ++i)

@@ -142,6 +142,7 @@ __global__ void __launch_bounds__(STEP_THREADS, LBM_TC_MINB)
   static_assert(STEP_THREADS == 128, "one MMA row per thread");
   __shared__ __align__(1024) uint8_t sA[2 * CLO_TILE_A_BYTES];
   __shared__ __align__(1024) uint8_t sB[CLO_HID * 64];
+  __shared__ __align__(1024) uint8_t sB1[CLO_HID * 64];  // W1 as a 32 x 32 tile, k >= 9 zero
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tslot;
   __shared__ uint32_t gave_up[STEP_THREADS / 32];
@@ -149,9 +150,12 @@ __global__ void __launch_bounds__(STEP_THREADS, LBM_TC_MINB)
   const int tid = threadIdx.y * 32 + threadIdx.x;
   if (tid < STEP_THREADS / 32) gave_up[tid] = 0u;
   if (tid == 0) last_phase = 0u;
-  for (int e = tid; e < CLO_HID * CLO_HID; e += STEP_THREADS)
-    *reinterpret_cast<__nv_bfloat16*>(sB + clo_tile_off(e / CLO_HID, e % CLO_HID)) =
-        __float2bfloat16_rn(net.v[CLO_W2 + e]);
+  for (int e = tid; e < CLO_HID * CLO_HID; e += STEP_THREADS) {
+    const int n = e / CLO_HID, k = e % CLO_HID;
+    *reinterpret_cast<__nv_bfloat16*>(sB + clo_tile_off(n, k)) = __float2bfloat16_rn(net.v[CLO_W2 + e]);
+    *reinterpret_cast<__nv_bfloat16*>(sB1 + clo_tile_off(n, k)) =
+        __float2bfloat16_rn(k < CLO_IN ? net.v[CLO_W1 + n * CLO_IN + k] : 0.0f);
+  }
   const uint32_t mbar_addr = (uint32_t)__cvta_generic_to_shared(&mbar);
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(mbar_addr), "r"(1) : "memory");
@@ -171,6 +175,7 @@ __global__ void __launch_bounds__(STEP_THREADS, LBM_TC_MINB)
   c.sA = sA;
   c.sA_addr = (uint32_t)__cvta_generic_to_shared(sA);
   c.sB_addr = (uint32_t)__cvta_generic_to_shared(sB);
+  c.sB1_addr = (uint32_t)__cvta_generic_to_shared(sB1);
   c.mbar_addr = mbar_addr;
   c.tmem = tslot;
   c.status = status;
