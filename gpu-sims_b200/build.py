@@ -84,12 +84,29 @@ def build(force: bool = False, verbose: bool = False, out: Path | None = None,
     return OUT
 
 
+HOST_SRC = PKG / "host" / "lbm_frame_loop.cpp"
+
+
+def build_host(lib: Path | None = None, out: Path | None = None) -> Path:
+    """Compiles the headless C++ host program (host/lbm_frame_loop.cpp)
+    against include/ and the library, with the library's directory as its
+    run path."""
+    lib = lib or OUT
+    out = out or HOST_SRC.with_suffix("")
+    cxx = shutil.which("g++") or "g++"
+    cmd = [cxx, "-std=c++17", "-O2", "-Wall", "-I", str(INCLUDE), str(HOST_SRC), "-o", str(out),
+           "-L", str(lib.parent), "-l:" + lib.name, "-Wl,-rpath," + str(lib.parent)]
+    subprocess.run(cmd, check=True)
+    return out
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
     ap.add_argument("-v", "--verbose", action="store_true")
     a = ap.parse_args()
     print(build(force=a.force, verbose=a.verbose))
+    print(build_host())
     return 0
 
 
