@@ -77,6 +77,30 @@ def test_batch_equals_single_domains(gpu, prec, coll):
             b.close()
 
 
+@pytest.mark.parametrize("persistent", [0, 1])
+def test_batch_matches_fp64_oracle(gpu, oracle, persistent):
+    """Every domain of a batch against the FP64 textbook step run alone
+    (ExtStep), at the physics-mode bar: |du| <= 3e-5 of the velocity scale,
+    |drho| <= 1e-5, after 120 steps (fp32 storage, BGK)."""
+    descs = domain_descs(gpu, 0, 0)
+    b = batch_of(gpu, descs)
+    b.set_schedule(rows_per_block=4, z_per_thread=2, persistent=persistent)
+    b.step(120)
+    b.sync()
+    for i, d in enumerate(descs):
+        mask, rho, u = initial_state(d, i)
+        shape = (d.nx, d.ny, d.nz)
+        wall = np.array([[d.wall_velocity[f][a] for a in range(3)] for f in range(6)])
+        st = oracle.ExtState(shape, periodic=tuple(d.periodic), tau=d.tau, collision=0, wall=wall, mask=mask)
+        st.init(rho.astype(np.float64), u.T.astype(np.float64))
+        st.step(120)
+        r2, u2 = b.read_moments(i)
+        scale = max(np.abs(st.u).max(), 1e-12)
+        assert np.abs(u2.T - st.u).max() / scale <= 3e-5, i
+        assert np.abs(r2 - st.rho).max() <= 1e-5, i
+    b.close()
+
+
 def test_persistent_barrier_timeout_is_reported(gpu):
     descs = domain_descs(gpu)
     b = batch_of(gpu, descs)
