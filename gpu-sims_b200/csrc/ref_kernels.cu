@@ -92,14 +92,21 @@ __device__ __forceinline__ void set_equilibrium(float (&g)[Q], float rho, float 
   static_for<0, Q>([&](auto I) { g[I.value] = rl_feq<decltype(I)::value>(rho, ux, uy, uz, uu); });
 }
 
-// One warp per block, the row (y, z) from blockIdx: the row terms of the
-// pulls are warp-uniform to the compiler (uniform datapath).
+// LBM_REF_WARPS warps per block side by side along x, the row (y, z) from
+// blockIdx: the row terms of the pulls are warp-uniform to the compiler
+// (uniform datapath).
+#ifndef LBM_REF_WARPS
+#define LBM_REF_WARPS 1
+#endif
+#ifndef LBM_REF_MINB
+#define LBM_REF_MINB (32 / LBM_REF_WARPS)
+#endif
 template <bool WRITE_MOMENTS>
-__global__ void __launch_bounds__(32, 32)
+__global__ void __launch_bounds__(32 * LBM_REF_WARPS, LBM_REF_MINB)
     k_ref_step(RefParams p, const float* __restrict__ fin, float* __restrict__ fout,
                const uint8_t* __restrict__ flags, const uint32_t* __restrict__ links,
                float* __restrict__ rho_o, float* __restrict__ u_o, unsigned* __restrict__ status) {
-  const int x = blockIdx.x * 32 + threadIdx.x;
+  const int x = (blockIdx.x * LBM_REF_WARPS + threadIdx.y) * 32 + threadIdx.x;
   const int y = blockIdx.y;
   const int z = blockIdx.z;
   if (x >= p.nx || y >= p.ny || z >= p.nz) return;
@@ -238,8 +245,11 @@ dim3 ref_grid(const RefParams& p) {
   const dim3 b = ref_block();
   return dim3((p.nx + b.x - 1) / b.x, (p.ny + b.y - 1) / b.y, (p.nz + b.z - 1) / b.z);
 }
-// k_ref_step: one warp of 32 x per block, a block per (x tile, y, z)
-dim3 row_grid(const RefParams& p) { return dim3((p.nx + 31) / 32, p.ny, p.nz); }
+// k_ref_step: LBM_REF_WARPS warps of 32 x per block, a block per (x tile, y, z)
+dim3 row_grid(const RefParams& p) {
+  return dim3((p.nx + 32 * LBM_REF_WARPS - 1) / (32 * LBM_REF_WARPS), p.ny, p.nz);
+}
+dim3 row_block() { return dim3(32, LBM_REF_WARPS, 1); }
 
 }  // namespace
 
@@ -256,9 +266,9 @@ cudaError_t ref_init(const Ctx& c, const float* rho, const float* u3, float rho0
 cudaError_t ref_step_with(const Ctx& c, const RefParams& p, const float* fin, float* fout,
                           bool write_moments, cudaStream_t s) {
   if (write_moments)
-    k_ref_step<true><<<row_grid(p), 32, 0, s>>>(p, fin, fout, c.flags, c.links, c.rho, c.u, c.status);
+    k_ref_step<true><<<row_grid(p), row_block(), 0, s>>>(p, fin, fout, c.flags, c.links, c.rho, c.u, c.status);
   else
-    k_ref_step<false><<<row_grid(p), 32, 0, s>>>(p, fin, fout, c.flags, c.links, c.rho, c.u, c.status);
+    k_ref_step<false><<<row_grid(p), row_block(), 0, s>>>(p, fin, fout, c.flags, c.links, c.rho, c.u, c.status);
   return cudaGetLastError();
 }
 
