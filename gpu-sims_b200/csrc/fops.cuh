@@ -8,10 +8,14 @@ namespace lbm {
 namespace {
 
 // Arithmetic policies for the collision.  Every operation is an explicitly
-// rounded intrinsic (no compiler contraction), so the one-node policy and
-// the two-node policy built on Blackwell's packed fp32 instructions
-// (FADD2/FMUL2/FFMA2: one instruction for two lanes' values) evaluate the
-// same operation graph and give bit-identical populations.
+// rounded intrinsic, so the one-node policy and the two-node policy built on
+// Blackwell's packed fp32 instructions (FADD2/FMUL2/FFMA2: one instruction
+// for two lanes' values) evaluate the same operation graph.  The scalar
+// intrinsics are never contracted; ptxas does merge a packed multiply into a
+// packed add that consumes it (even when both carry an explicit .rn, and
+// with ptxas contraction switched off), so the two policies agree bit for
+// bit where the code is fma-shaped, and otherwise to within an ulp per
+// merged pair.
 struct Ops1 {
   using F = float;
   static __device__ __forceinline__ F splat(float c) { return c; }
