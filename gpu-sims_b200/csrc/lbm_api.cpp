@@ -322,8 +322,7 @@ int lbm_set_step_variant(lbm_ctx* c, int nodes_per_thread) {
   if (c->d.mode != LBM_MODE_PHYSICS && v != 0)
     return fail(c, LBM_ERR_UNSUPPORTED, "step variants are physics-mode kernels");
   if (v == 2 && c->d.nx % 2) return fail(c, LBM_ERR_UNSUPPORTED, "two nodes per thread need an even nx");
-  if (v == 4 && (c->d.nx % 4 || c->d.precision == LBM_PREC_F32))
-    return fail(c, LBM_ERR_UNSUPPORTED, "four nodes per thread need nx % 4 == 0 and 2-byte storage");
+  if (v == 4 && c->d.nx % 4) return fail(c, LBM_ERR_UNSUPPORTED, "four nodes per thread need nx % 4 == 0");
   if ((v == 4 || v == 8) && c->pp.any_open)
     return fail(c, LBM_ERR_UNSUPPORTED, "open x faces run with one or two nodes per thread");
   CK(cudaStreamSynchronize(c->stream), "set_step_variant sync");

@@ -896,6 +896,17 @@ __device__ __forceinline__ void step_row2(const PhysParams& p, const CloNet<SGS>
 
 // Four x-adjacent 2-byte slots as one 8-byte access (x a multiple of 4).
 template <int PREC> struct Vec4;
+template <> struct Vec4<LBM_PREC_F32> {  // one 16-byte access per slot quad
+  using T = float;
+  static __device__ __forceinline__ float4 ld(const T* p, uint32_t i) {
+    return *reinterpret_cast<const float4*>(p + i);
+  }
+  static __device__ __forceinline__ float2 lo(float4 v) { return make_float2(v.x, v.y); }
+  static __device__ __forceinline__ float2 hi(float4 v) { return make_float2(v.z, v.w); }
+  static __device__ __forceinline__ void st(T* p, uint32_t i, float2 l, float2 h) {
+    *reinterpret_cast<float4*>(p + i) = make_float4(l.x, l.y, h.x, h.y);
+  }
+};
 template <> struct Vec4<LBM_PREC_F16S> {
   using T = __half;
   static __device__ __forceinline__ uint2 ld(const T* p, uint32_t i) { return *reinterpret_cast<const uint2*>(p + i); }
@@ -927,10 +938,11 @@ template <> struct Vec4<LBM_PREC_BF16S> {
   }
 };
 
-// Four nodes per thread for the 2-byte formats (fp16 / bf16 shifted
-// storage), nx a multiple of 4: lane l updates x = x0 + 4l .. x + 3 (nodes A,
-// B, C, D); a warp covers 128 consecutive x.  The same scheme as step_row2
-// with 8-byte accesses: every slot quad moves as one access, the slots at
+// Four nodes per thread, nx a multiple of 4: lane l updates x = x0 + 4l ..
+// x + 3 (nodes A, B, C, D); a warp covers 128 consecutive x.  The same scheme
+// as step_row2 with 8-byte (2-byte formats) or 16-byte (fp32) accesses:
+// every slot quad moves as one access (x = 4l and rows padded to multiples of
+// 8 slots keep it aligned), the slots at
 // x+1 .. x+4 of the c_x = +1 pairs come from the lane's own vector and the
 // next lane's first element by one shuffle, the row's last quad touching
 // x+4 itself; A+B and C+D collide as two packed pairs (Ops2), so results are
@@ -970,7 +982,7 @@ __device__ __forceinline__ void step_row4(const PhysParams& p, const CloNet<SGS>
   const uint32_t fl4 = valid ? *reinterpret_cast<const uint32_t*>(flags + nid) : 0x01010101u;
   float2 gl[Q], gh[Q];  // gl: .x = A, .y = B;  gh: .x = C, .y = D
   {
-    const uint2 r = V4::ld(pop, lnA);
+    const auto r = V4::ld(pop, lnA);
     gl[0] = V4::lo(r);
     gh[0] = V4::hi(r);
   }
@@ -984,12 +996,12 @@ __device__ __forceinline__ void step_row4(const PhysParams& p, const CloNet<SGS>
     const bool yz_fwd = (DY > 0 && yhi) || (DY < 0 && ylo) || (DZ > 0 && zhi) || (DZ < 0 && zlo);
     const bool yz_bwd = (DY > 0 && ylo) || (DY < 0 && yhi) || (DZ > 0 && zlo) || (DZ < 0 && zhi);
     // f_a of the four nodes from X = S[1-P](x..x+3); S[P] across a wall
-    const uint2 xv = V4::ld(yz_bwd ? sP : sQ, lnA);
+    const auto xv = V4::ld(yz_bwd ? sP : sQ, lnA);
     gl[a] = V4::lo(xv);
     gh[a] = V4::hi(xv);
     if (DX > 0 && xloA) gl[a].x = S::raw_ld(sP, lnA);  // node A at the -x wall
     // f_b from Y = S[P](n + d); S[1-P] across a wall
-    const uint2 yv = V4::ld(yz_fwd ? sQ : sP, lnA + offs<0, DY, DZ>(G, w));
+    const auto yv = V4::ld(yz_fwd ? sQ : sP, lnA + offs<0, DY, DZ>(G, w));
     const float2 ylo2 = V4::lo(yv), yhi2 = V4::hi(yv);
     if (DX == 0) {
       gl[b] = ylo2;

@@ -104,17 +104,28 @@ __global__ void __launch_bounds__(128)
 #ifndef LBM_STEP4_MINB
 #define LBM_STEP4_MINB 4  // x STEP_BY / LBM_STEP4_ROWS blocks per SM
 #endif
+// fp32 storage (16-byte slot quads), channel 512x128x128 with a body force,
+// against 38.4 GLUPS for the two-node kernel: 16 blocks per SM 37.9 GLUPS
+// (128 registers, 124 bytes spilled in the forced kernel), 12 blocks 36.6 (168,
+// no spills), 8 blocks 27.8.  The automatic choice stays at two nodes.
+#ifndef LBM_STEP4_MINB32
+#define LBM_STEP4_MINB32 4
+#endif
 
-// Four nodes per thread (2-byte storage, nx % 4 == 0): a warp covers 128 x,
-// in one-warp blocks (row = blockIdx.y, warp-uniform), 16 per SM (127
+// Four nodes per thread (nx % 4 == 0): a warp covers 128 x, in one-warp
+// blocks (row = blockIdx.y, warp-uniform).  2-byte storage: 16 per SM (127
 // registers, no spills).  Measured on B200, channel 512x128x128 fp16: 53.8
 // GLUPS against 47.6 with four-row blocks and 49.9 with 12 one-warp blocks per
 // SM (which spilled 36 bytes); the two-node kernel runs 54.1.
 #ifndef LBM_STEP4_ROWS
 #define LBM_STEP4_ROWS 1
 #endif
+template <int PREC>
+constexpr int step4_minb() {
+  return (PREC == LBM_PREC_F32 ? LBM_STEP4_MINB32 : LBM_STEP4_MINB) * STEP_BY / LBM_STEP4_ROWS;
+}
 template <int PREC, int COLL, int SGS, bool FORCE, bool WRITE_MOMENTS, int P>
-__global__ void __launch_bounds__(32 * LBM_STEP4_ROWS, LBM_STEP4_MINB * STEP_BY / LBM_STEP4_ROWS)
+__global__ void __launch_bounds__(32 * LBM_STEP4_ROWS, step4_minb<PREC>())
     k_phys_step4(PhysParams p, void* __restrict__ pop_v, const uint8_t* __restrict__ flags,
                  const uint32_t* __restrict__ links, float* __restrict__ rho_o,
                  float* __restrict__ u_o, unsigned* __restrict__ status,
@@ -236,11 +247,11 @@ template <> CloNet<2> net_of<2>(const Ctx& c) {
 }
 
 // Nodes per thread: the context's choice (lbm_set_step_variant) or, by
-// default, four for the 2-byte formats when step_quads(nx), two when
+// default, four when step_quads(nx) (a build option), two when
 // step_pairs(nx), else one.
 inline bool use_quads(const Ctx& c) {
   const int nx = c.pp.g.nx;
-  if (c.d.precision == LBM_PREC_F32 || c.closure || c.pp.any_open || nx % 4) return false;
+  if (c.closure || c.pp.any_open || nx % 4) return false;
   return c.step_variant == 4 || (c.step_variant == 0 && step_quads(nx));
 }
 inline bool use_pairs(const Ctx& c) {
@@ -254,7 +265,7 @@ cudaError_t launch_rows(const Ctx& c, int P, bool wm, cudaStream_t s) {
   const PhysGeom& G = c.pp.g;
   const CloNet<SGS> net = net_of<SGS>(c);
   const dim3 blk(32, STEP_BY, 1);
-  if constexpr (PREC != LBM_PREC_F32 && SGS != 2) {
+  if constexpr (SGS != 2) {
     if (use_quads(c)) {
       constexpr int R4 = LBM_STEP4_ROWS;
       const dim3 grd((G.nx + 127) / 128, (G.ny + R4 - 1) / R4, G.nz), blk4(32, R4, 1);

@@ -196,7 +196,8 @@ LBM_API int lbm_step(lbm_ctx* ctx, int nsteps);
 
 /* Physics mode: kernel variant of the step.  0 = automatic (two nodes per
  * thread when nx is even and the rows fill 64-wide warps, else one); 1, 2 or
- * 4 nodes per thread (4: fp16/bf16 storage and nx % 4 == 0); 8 = one node per
+ * 4 nodes per thread (4: nx % 4 == 0; one 16-byte access per slot quad for
+ * fp32 storage, 8-byte for fp16/bf16); 8 = one node per
  * thread with the learned closure's hidden layer on the tensor cores (tcgen05;
  * without a closure the same as 1).  The 1-, 2- and 4-node variants agree bit
  * for bit except with a body force, where the one-node kernel's force terms

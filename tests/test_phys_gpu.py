@@ -172,19 +172,19 @@ def test_set_flags_requires_reinit(gpu):
     lat.close()
 
 
-@pytest.mark.parametrize("prec", [1, 2])
+@pytest.mark.parametrize("prec", [0, 1, 2])
 @pytest.mark.parametrize("case", ["walls", "periodic", "periodic_force", "smag"])
 def test_step_variants_bit_identical(gpu, prec, case):
     """Two and four nodes per thread run the same packed operations: their
-    stored populations and moments agree bit for bit (fp16 / bf16 storage,
-    where four nodes per thread exist), across x walls, a moving lid, an
-    interior sphere, periodic wrap, TRT and Smagorinsky.  The one-node
+    stored populations and moments agree bit for bit (fp32 storage with
+    16-byte slot quads, fp16 / bf16 with 8-byte ones), across x walls, a
+    moving lid, an interior sphere, periodic wrap, TRT and Smagorinsky.  The one-node
     kernel agrees bit for bit too, except with a body force, where its
     scalar code path and the packed path's compiled force terms differ by
     at most a few units in the last place of fp32 in a few per cent of values,
     which flips the rounding of some stored fp16 / bf16 values (the stated bar
-    there after 50 steps: 1e-3 of the velocity scale for fp16, 1e-2 for bf16's
-    8-bit mantissa)."""
+    there after 50 steps: 1e-4 of the velocity scale for fp32, 1e-3 for fp16,
+    1e-2 for bf16's 8-bit mantissa)."""
     if case == "walls":
         shape, kw = (40, 12, 10), dict(periodic=(0, 0, 0), collision=0, tau=0.6)
         wall = np.zeros((6, 3))
@@ -219,7 +219,7 @@ def test_step_variants_bit_identical(gpu, prec, case):
     assert np.array_equal(g2, g4) and np.array_equal(r2, r4) and np.array_equal(u2, u4)
     g1, r1, u1 = out[1]
     if case == "periodic_force":
-        bar = 1e-3 if prec == gpu.PREC_F16S else 1e-2
+        bar = {gpu.PREC_F32: 1e-4, gpu.PREC_F16S: 1e-3}.get(prec, 1e-2)
         assert np.max(np.abs(u1 - u2)) <= bar * np.abs(u2).max()
     else:
         assert np.array_equal(g1, g2) and np.array_equal(r1, r2) and np.array_equal(u1, u2)
@@ -234,6 +234,9 @@ def test_step_variant_rules(gpu):
         lat.set_step_variant(3)
     lat.close()
     lat = gpu.Lattice(nx=32, ny=8, nz=8, mode=gpu.MODE_PHYSICS)
+    lat.set_step_variant(4)  # fp32 storage: 16-byte slot quads
+    lat.close()
+    lat = gpu.Lattice(nx=30, ny=8, nz=8, mode=gpu.MODE_PHYSICS)
     with pytest.raises(gpu.LbmError):
-        lat.set_step_variant(4)  # fp32 storage
+        lat.set_step_variant(4)
     lat.close()
