@@ -142,15 +142,19 @@ __global__ void __launch_bounds__(32 * LBM_STEP4_ROWS, step4_minb<PREC>())
 // walks LBM_TC_ZPB planes so that its set-up (the 32-column TMEM allocation,
 // the bf16 W2 tile, the mbarrier) is paid once per several MMAs.  Rows
 // beyond ny run on the last row without storing, so every thread reaches the
-// CTA-wide barriers.
+// CTA-wide barriers.  At four CTAs per SM, 128^3: 16 planes 14.5 / 15.8
+// GLUPS (fp32 / fp16 storage), 8 planes 14.3 / 15.6, 4 planes 13.6 / 14.8.
 #ifndef LBM_TC_ZPB
-#define LBM_TC_ZPB 8
+#define LBM_TC_ZPB 16
 #endif
-// Two CTAs per SM: the kernel then keeps its 168 registers without spills
-// and runs 10.8 / 12.6 GLUPS (fp32 / fp16 storage, 128^3) against 9.0 / 9.7
-// at three CTAs per SM (spilling) and 10.2 / 11.2 for the CUDA-core MLP.
+// Four CTAs per SM (124 registers, no spills): 14.3 / 15.5 GLUPS (fp32 /
+// fp16 storage, 128^3) against 12.5 / 14.1 with the three CTAs that 149
+// registers allow.  The kernel is bound by dependent-instruction latency
+// (MMA waits, barriers, the feature chain) at a few warps per scheduler, so
+// residency pays more than instruction count.  (Before the first layer moved
+// to the tensor cores the kernel needed 168 registers and spilled at three.)
 #ifndef LBM_TC_MINB
-#define LBM_TC_MINB 2
+#define LBM_TC_MINB 4
 #endif
 template <int PREC, int COLL, bool WRITE_MOMENTS, int P>
 __global__ void __launch_bounds__(STEP_THREADS, LBM_TC_MINB)
