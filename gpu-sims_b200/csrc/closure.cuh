@@ -42,7 +42,7 @@ template <> struct CloNet<2> {
 // cores.  Built by k_phys_step_tc (phys_step_launch.cuh), which owns the
 // shared tiles, the mbarrier and the TMEM columns.
 //
-// A wait for an MMA that runs out (LBM_CLO_WAIT_LIMIT polls) must not leave
+// A wait for an MMA that runs out (wait_limit polls) must not leave
 // the tensor core reading a tile that the CTA goes on to rewrite.  So the A
 // tile is double-buffered by phase, a warp that gives up marks its entry of
 // `gave_up` (shared, sticky), and every later evaluation starts with a
@@ -58,6 +58,7 @@ template <> struct CloNet<3> {
   unsigned* status;
   uint32_t* gave_up;        // shared, one word per warp: that warp's wait ran out
   uint32_t* last_phase;     // shared: phase of the last MMA commit issued
+  uint32_t wait_limit;      // polls per MMA wait before the CTA gives up
   bool row_ok;              // this thread's row exists (y < ny)
   uint32_t phase;           // mbarrier phase of this evaluation (alternates per use)
   __device__ __forceinline__ float operator[](int k) const { return net->v[k]; }
@@ -86,10 +87,6 @@ constexpr uint32_t CLO_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((32u >> 3) 
 __host__ __device__ constexpr uint32_t clo_tile_off(int row, int k) {
   return (uint32_t)((row >> 3) * 512 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
 }
-// bound of the wait for the MMA: the kernel reports LBM_ERR_TIMEOUT past it
-#ifndef LBM_CLO_WAIT_LIMIT
-#define LBM_CLO_WAIT_LIMIT (1 << 22)
-#endif
 
 namespace {
 
@@ -155,7 +152,7 @@ __device__ __forceinline__ typename O::F closure_mlp(const W& w, const typename 
 // completed, per warp (the tensor-memory load after it is warp-collective).
 __device__ __forceinline__ bool clo_wait(const CloNet<3>& c, uint32_t parity) {
   uint32_t done = 0;
-  for (int it = 0; it < LBM_CLO_WAIT_LIMIT && !done; ++it)
+  for (uint32_t it = 0; it < c.wait_limit && !done; ++it)
     asm volatile(
         "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
         "selp.b32 %0, 1, 0, P1;\n\t}\n"

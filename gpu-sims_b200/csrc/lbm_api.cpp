@@ -352,6 +352,15 @@ int lbm_set_closure(lbm_ctx* c, const float* net) {
   return c->initialized ? prepare_graphs(c) : LBM_OK;
 }
 
+int lbm_set_closure_wait_limit(lbm_ctx* c, int32_t polls) {
+  if (int rc = check_ctx(c)) return rc;
+  // the bound is a launch argument of the captured step graphs: rebuild them
+  CK(cudaStreamSynchronize(c->stream), "set_closure_wait_limit sync");
+  drop_graphs(c);
+  c->clo_wait_polls = polls < 0 ? (uint32_t)LBM_CLO_WAIT_LIMIT : (uint32_t)polls;
+  return c->initialized ? prepare_graphs(c) : LBM_OK;
+}
+
 // Classifies the mask already in c->mask (lbm_set_flags, lbm_set_flags_naca).
 static int classify_mask(lbm_ctx* c) {
   const int per[3] = {c->d.mode == LBM_MODE_PHYSICS ? c->d.periodic[0] : 0,

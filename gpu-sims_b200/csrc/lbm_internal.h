@@ -61,6 +61,12 @@ struct PhysGeom {
   size_t slot_stride;  // elements per slot array
 };
 
+// default bound of the tensor-core closure's wait for its MMA (lbm_set_closure_wait_limit sets
+// another): the kernel reports LBM_ERR_TIMEOUT past it
+#ifndef LBM_CLO_WAIT_LIMIT
+#define LBM_CLO_WAIT_LIMIT (1 << 22)
+#endif
+
 struct PhysParams {
   PhysGeom g;
   float omega;         // 1/tau
@@ -159,6 +165,7 @@ struct Ctx {
   // value; weights already rounded to bf16
   bool closure = false;
   float clo[LBM_CLOSURE_FLOATS] = {};
+  uint32_t clo_wait_polls = LBM_CLO_WAIT_LIMIT;  // polls per tensor-core MMA wait
   // nodes per thread of the physics step: 0 automatic, 1, 2 or 4
   int step_variant = 0;
   bool initialized = false;

@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(STEP_THREADS, LBM_TC_MINB)
     k_phys_step_tc(PhysParams p, void* __restrict__ pop_v, const uint8_t* __restrict__ flags,
                    const uint32_t* __restrict__ links, float* __restrict__ rho_o,
                    float* __restrict__ u_o, unsigned* __restrict__ status,
-                   const __grid_constant__ CloNet<2> net) {
+                   const __grid_constant__ CloNet<2> net, uint32_t wait_polls) {
   static_assert(STEP_THREADS == 128, "one MMA row per thread");
   __shared__ __align__(1024) uint8_t sA[2 * CLO_TILE_A_BYTES];
   __shared__ __align__(1024) uint8_t sB[CLO_HID * 64];
@@ -204,6 +204,7 @@ __global__ void __launch_bounds__(STEP_THREADS, LBM_TC_MINB)
   c.status = status;
   c.gave_up = gave_up;
   c.last_phase = &last_phase;
+  c.wait_limit = wait_polls;
   c.row_ok = y < p.g.ny;
   const int z0 = blockIdx.z * LBM_TC_ZPB;
   const int z1 = min(p.g.nz, z0 + LBM_TC_ZPB);  // uniform over the CTA
@@ -229,7 +230,8 @@ __global__ void __launch_bounds__(STEP_THREADS, LBM_TC_MINB)
   if (threadIdx.y == 0) {
     if (aborted) {
       // the last MMA whose wait ran out may still run: wait for its commit
-      // (bounded) before its tensor memory is freed
+      // (bounded, always by the default limit, whatever the per-plane
+      // bound) before its tensor memory is freed
       uint32_t done = 0;
       for (int it = 0; it < LBM_CLO_WAIT_LIMIT && !done; ++it)
         asm volatile(
@@ -347,7 +349,8 @@ cudaError_t launch_step_tc(const Ctx& c, int P, bool wm, cudaStream_t s) {
   const dim3 grd((G.nx + 31) / 32, (G.ny + STEP_BY - 1) / STEP_BY, (G.nz + LBM_TC_ZPB - 1) / LBM_TC_ZPB);
 #define LBM_STEP_LAUNCH(WM, PAR)                                          \
   k_phys_step_tc<PREC, COLL, WM, PAR><<<grd, blk, 0, s>>>(                \
-      c.pp, c.pop, c.flags, c.links, c.rho, c.u, c.status, net)
+      c.pp, c.pop, c.flags, c.links, c.rho, c.u, c.status, net, polls)
+  const uint32_t polls = c.clo_wait_polls;
   if (wm) {
     if (P) LBM_STEP_LAUNCH(true, 1); else LBM_STEP_LAUNCH(true, 0);
   } else {
@@ -361,8 +364,8 @@ cudaError_t launch_step_tc(const Ctx& c, int P, bool wm, cudaStream_t s) {
 // force, which lbm_set_closure enforces): the CUDA-core MLP (one or two
 // nodes per thread, fp32 activations) by default, the tensor-core MLP (bf16
 // hidden activations) for variant 8.  Measured on B200 at 128^3: CUDA-core
-// pair kernel 10.2 / 11.2 GLUPS (fp32 / fp16 storage), tensor-core kernel
-// 10.8 / 12.6.
+// pair kernel 10.5 / 11.9 GLUPS (fp32 / fp16 storage), tensor-core kernel
+// 14.5 / 15.8.
 template <int PREC, int COLL, bool CLOSURE>
 cudaError_t dispatch_smag(const Ctx& c, int P, bool wm, cudaStream_t s) {
   if constexpr (CLOSURE) {

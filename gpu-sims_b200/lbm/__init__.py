@@ -222,6 +222,7 @@ _SIGS = {
     "lbm_colormap_lut": (C.c_int, [_P]),
     "lbm_jitter_lut": (C.c_int, [_P]),
     "lbm_set_closure": (C.c_int, [_P, _P]),
+    "lbm_set_closure_wait_limit": (C.c_int, [_P, C.c_int32]),
     "lbm_box_filter": (C.c_int, [_P, _P, _I32, _I32, _I32, _I32, _P, _P]),
     "lbm_closure_samples": (C.c_int, [_P, _I32, _I32, _I32, _F, _F, _U64, _I64, _P, _P, _P, _P]),
     "lbm_closure_predict": (C.c_int, [_P, _P, _I64, _P, _P]),
@@ -446,6 +447,11 @@ class Lattice:
         if w.size != CLOSURE_FLOATS:
             raise LbmError(ERR_INVALID_ARG, f"network must have {CLOSURE_FLOATS} floats")
         self._c(load().lbm_set_closure(self._h, _ptr(w)))
+
+    def set_closure_wait_limit(self, polls: int) -> None:
+        """Testing hook: polls per tensor-core MMA wait (< 0: the default,
+        0: give up at once); see lbm_set_closure_wait_limit."""
+        self._c(load().lbm_set_closure_wait_limit(self._h, int(polls)))
 
     def read_classification(self) -> np.ndarray:
         out = np.zeros(self.n, np.uint32)

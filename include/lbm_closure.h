@@ -56,6 +56,17 @@ extern "C" {
  * and weights, fp32 accumulator in tensor memory). */
 LBM_API int lbm_set_closure(lbm_ctx* ctx, const float* net);
 
+/* Testing hook of the tensor-core closure step (variant 8): the bound, in
+ * polls of mbarrier.try_wait (each of which the hardware may suspend for a
+ * while), of each wait for the CTA's MMAs; polls < 0 restores the default
+ * (2^22), 0 makes every such wait give up at once.  A wait that runs out
+ * makes that CTA issue no further MMA in the launch: its nodes fall back to
+ * r = 1 (plain Smagorinsky) and lbm_sync reports LBM_ERR_TIMEOUT.  The wait
+ * that keeps a CTA from freeing its tensor memory under an MMA still in
+ * flight keeps the default bound, so 0 exercises the give-up path without a
+ * fault.  Takes effect at the next step; the context stays usable. */
+LBM_API int lbm_set_closure_wait_limit(lbm_ctx* ctx, int32_t polls);
+
 /* Box filter of moment fields by `factor` along each axis (factor divides
  * nx, ny, nz).  d_rho float[n], d_u float[3][n] planes (as from
  * lbm_device_moments); d_out float[10][nc] planes, nc = n / factor^3, in the

@@ -366,3 +366,48 @@ def test_tensor_core_mlp_matches_cuda_core_mlp(gpu, oracle, shape):
     assert np.max(np.abs(runs[0].T - st.u)) / scale <= 1e-4  # tensor cores
     assert np.max(np.abs(runs[0] - runs[1])) / scale <= 1e-4
     assert not np.array_equal(runs[0], runs[1])  # the two paths really differ
+
+
+def test_tensor_core_wait_gives_up_without_a_fault(gpu):
+    """The tensor-core closure's bounded MMA wait, made to run out on the GPU
+    (no poll per wait, lbm_set_closure_wait_limit; a single try_wait may
+    already be suspended until the small MMA completes) with no fault: lbm_sync
+    reports LBM_ERR_TIMEOUT, the state stays finite (the CTAs that gave up
+    took r = 1, plain Smagorinsky), and the context stays usable -- with the
+    default bound restored and the same initial state, 20 steps (a graph of
+    16 and four single launches) equal a fresh context's bit for bit."""
+    shape = (64, 32, 32)
+    n = int(np.prod(shape))
+    net = _net(13)
+    u = np.ascontiguousarray(_smooth_field(shape, 1).astype(np.float32).T)
+    rho = np.ones(n, np.float32)
+
+    def lattice():
+        d = gpu.default_desc(nx=shape[0], ny=shape[1], nz=shape[2], mode=gpu.MODE_PHYSICS,
+                             periodic=(1, 1, 1), tau=0.52, smagorinsky_cs=0.15)
+        lat = gpu.Lattice(d)
+        lat.set_closure(net)
+        lat.set_step_variant(8)
+        lat.init_from_moments(rho, u)
+        return lat
+
+    fresh = lattice()
+    fresh.step(20)
+    fresh.sync()
+    want = fresh.read_populations_shifted()
+    fresh.close()
+
+    lat = lattice()
+    lat.set_closure_wait_limit(0)
+    lat.step(20)
+    with pytest.raises(gpu.LbmError) as e:
+        lat.sync()
+    assert e.value.code == gpu.ERR_TIMEOUT
+    _, u_gave_up = lat.read_moments()
+    assert np.isfinite(u_gave_up).all()
+    lat.set_closure_wait_limit(-1)
+    lat.init_from_moments(rho, u)
+    lat.step(20)
+    lat.sync()
+    assert np.array_equal(lat.read_populations_shifted(), want)
+    lat.close()
