@@ -85,8 +85,8 @@ class ClockSampler:
     REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
                0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
 
-    # 0.5 ms: the driver's 20-step timed region lasts a few milliseconds (the
-    # timed calls release the GIL, so this thread polls while they run)
+    # polled as fast as NVML answers: a 20-step timed region lasts a few
+    # milliseconds
     def __init__(self, index: int, period: float = 0.0005):
         self.index, self.period = index, period
         self.samples, self.reasons = [], set()

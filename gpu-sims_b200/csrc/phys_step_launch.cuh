@@ -20,8 +20,15 @@ namespace {
 #ifndef LBM_CLO_MINB
 #define LBM_CLO_MINB 3
 #endif
+// The pair kernel with the CUDA-core MLP, 128^3: fp32 storage at three
+// blocks per SM (168 registers, 32-124 bytes spilled) 11.3 GLUPS against 10.5
+// at two (208-220 registers, no spills); the 2-byte formats 11.7 against 11.9,
+// so they keep two.
 #ifndef LBM_CLO2_MINB
 #define LBM_CLO2_MINB 2
+#endif
+#ifndef LBM_CLO2_MINB32
+#define LBM_CLO2_MINB32 3
 #endif
 
 // Rows per block of the pair kernel.  One-warp blocks whose row is
@@ -44,7 +51,7 @@ constexpr int step2_rows() {
 // SGS: 0 none, 1 Smagorinsky, 2 learned closure (net = the network).
 template <int PREC, int COLL, int SGS, bool FORCE, bool WRITE_MOMENTS, int P>
 __global__ void __launch_bounds__(32 * step2_rows<PREC, SGS>(),
-                                  SGS == 2 ? LBM_CLO2_MINB
+                                  SGS == 2 ? (PREC == LBM_PREC_F32 ? LBM_CLO2_MINB32 : LBM_CLO2_MINB)
                                            : (PREC == LBM_PREC_F32 ? LBM_STEP2_MINB * STEP_BY
                                                                    : LBM_STEP2_MINB16 * STEP_BY /
                                                                          LBM_STEP2_ROWS16))
@@ -364,7 +371,7 @@ cudaError_t launch_step_tc(const Ctx& c, int P, bool wm, cudaStream_t s) {
 // force, which lbm_set_closure enforces): the CUDA-core MLP (one or two
 // nodes per thread, fp32 activations) by default, the tensor-core MLP (bf16
 // hidden activations) for variant 8.  Measured on B200 at 128^3: CUDA-core
-// pair kernel 10.5 / 11.9 GLUPS (fp32 / fp16 storage), tensor-core kernel
+// pair kernel 11.3 / 11.9 GLUPS (fp32 / fp16 storage), tensor-core kernel
 // 14.5 / 15.8.
 template <int PREC, int COLL, bool CLOSURE>
 cudaError_t dispatch_smag(const Ctx& c, int P, bool wm, cudaStream_t s) {
