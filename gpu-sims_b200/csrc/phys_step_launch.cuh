@@ -7,13 +7,29 @@
 namespace lbm {
 namespace {
 
+// Residency of the pair kernel, x STEP_BY one-warp blocks per SM.  fp32
+// without Smagorinsky: 24 blocks (80 registers, up to ~100 bytes spilled in
+// the forced / moment-writing forms) against 20 (94 registers, no spills),
+// measured on B200: channel 512x128x128 39.3 vs 38.4 GLUPS, periodic TRT
+// 256^3 40.4 vs 37.7, lid cavity 192^3 38.8 vs 36.7.  With Smagorinsky the
+// same bound spills 280-340 bytes and loses (128^3: 28.3 vs 32.8), so the
+// Smagorinsky forms have their own bound: fp32 20 blocks (128^3 / 256^3 BGK /
+// 256^3 TRT: 32.7 / 34.7 / 32.6 GLUPS against 30.2 / 31.7 / 31.0 at 16); fp16
+// storage 20 blocks (128^3 BGK / 256^3 TRT: 45.2 / 41.5 against 43.0 / 38.9
+// at 24 and 47.1 / 35.0 at 16).
 #ifndef LBM_STEP2_MINB
-#define LBM_STEP2_MINB 5
+#define LBM_STEP2_MINB 6
+#endif
+#ifndef LBM_STEP2_MINB_SMAG
+#define LBM_STEP2_MINB_SMAG 5
 #endif
 // the 2-byte formats are issue-bound rather than memory-bound: their
-// residency bound is tuned separately
+// residency bounds are tuned separately
 #ifndef LBM_STEP2_MINB16
 #define LBM_STEP2_MINB16 6
+#endif
+#ifndef LBM_STEP2_MINB16_SMAG
+#define LBM_STEP2_MINB16_SMAG 5
 #endif
 // Residency bounds of the learned-closure kernels (the MLP's hidden layer
 // stays in registers: two nodes' worth in the pair kernel).
@@ -52,9 +68,10 @@ constexpr int step2_rows() {
 template <int PREC, int COLL, int SGS, bool FORCE, bool WRITE_MOMENTS, int P>
 __global__ void __launch_bounds__(32 * step2_rows<PREC, SGS>(),
                                   SGS == 2 ? (PREC == LBM_PREC_F32 ? LBM_CLO2_MINB32 : LBM_CLO2_MINB)
-                                           : (PREC == LBM_PREC_F32 ? LBM_STEP2_MINB * STEP_BY
-                                                                   : LBM_STEP2_MINB16 * STEP_BY /
-                                                                         LBM_STEP2_ROWS16))
+                                  : PREC == LBM_PREC_F32
+                                      ? (SGS == 1 ? LBM_STEP2_MINB_SMAG : LBM_STEP2_MINB) * STEP_BY
+                                      : (SGS == 1 ? LBM_STEP2_MINB16_SMAG : LBM_STEP2_MINB16) * STEP_BY /
+                                            LBM_STEP2_ROWS16)
     k_phys_step2(PhysParams p, void* __restrict__ pop_v, const uint8_t* __restrict__ flags,
                  const uint32_t* __restrict__ links, float* __restrict__ rho_o,
                  float* __restrict__ u_o, unsigned* __restrict__ status,
