@@ -273,7 +273,7 @@ class ExtStateGPU:
 
     def init(self, rho, u):
         t = self.torch
-        r = t.from_numpy(np.ascontiguousarray(np.broadcast_to(rho, (self.n,)), np.float64)).cuda()
+        r = t.from_numpy(np.array(np.broadcast_to(rho, (self.n,)), np.float64)).cuda()  # a writable copy
         uu = t.from_numpy(np.ascontiguousarray(np.asarray(u, np.float64).reshape(3, -1) * np.ones((3, self.n)))).cuda()
         t.cuda.synchronize()
         rc = lib_gpu().oracle_gpu_ext_init_f64(self.ip.ctypes.data, self.dp.ctypes.data, self.mask.data_ptr(),
