@@ -165,6 +165,7 @@ bool setup_physics(Ctx& c, const lbm_desc& d) {
   p.tau = d.tau;
   p.omega = 1.0f / d.tau;
   p.trt_magic = d.trt_magic;
+  p.omega_m = 1.0f / (p.trt_magic / (1.0f / p.omega - 0.5f) + 0.5f);
   p.smag_cs = d.smagorinsky_cs;
   for (int a = 0; a < 3; ++a) p.accel[a] = d.body_accel[a];
   p.any_moving_wall = 0;

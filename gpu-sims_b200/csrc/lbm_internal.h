@@ -70,6 +70,10 @@ struct PhysGeom {
 struct PhysParams {
   PhysGeom g;
   float omega;         // 1/tau
+  // TRT antisymmetric rate 1 / (trt_magic / (1/omega - 1/2) + 1/2) for that
+  // omega, evaluated once on the host with the step's own float operations
+  // (steps with Smagorinsky compute it per node from their local omega)
+  float omega_m;
   float tau;
   float trt_magic;
   float smag_cs;

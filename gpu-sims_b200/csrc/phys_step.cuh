@@ -227,7 +227,9 @@ __device__ __forceinline__ void collide_t(const PhysParams& p, const CloNet<SGS>
     omega = O::div(O::splat(1.0f), tau_eff);
   }
   F omega_m = omega;
-  if (COLL == LBM_COLL_TRT)
+  if (COLL == LBM_COLL_TRT && SGS == 0)
+    omega_m = O::splat(p.omega_m);  // the same operations, done once on the host
+  else if (COLL == LBM_COLL_TRT)
     omega_m = O::div(O::splat(1.0f),
                      O::add(O::div(O::splat(p.trt_magic),
                                    O::sub(O::div(O::splat(1.0f), omega), O::splat(0.5f))),
