@@ -24,6 +24,8 @@ struct Ops1 {
   static __device__ __forceinline__ F mul(F a, F b) { return __fmul_rn(a, b); }
   static __device__ __forceinline__ F fma(F a, F b, F c) { return __fmaf_rn(a, b, c); }
   static __device__ __forceinline__ F div(F a, F b) { return __fdiv_rn(a, b); }
+  // a / b to about 2 ulp (CUDA's fast division; b of order 1 here)
+  static __device__ __forceinline__ F div_fast(F a, F b) { return __fdividef(a, b); }
   static __device__ __forceinline__ F sqrt(F a) { return __fsqrt_rn(a); }
   static __device__ __forceinline__ F log(F a) { return logf(a); }
   static __device__ __forceinline__ F relu(F a) { return fmaxf(a, 0.0f); }
@@ -41,6 +43,9 @@ struct Ops2 {
   static __device__ __forceinline__ F fma(F a, F b, F c) { return __ffma2_rn(a, b, c); }
   static __device__ __forceinline__ F div(F a, F b) {
     return make_float2(__fdiv_rn(a.x, b.x), __fdiv_rn(a.y, b.y));
+  }
+  static __device__ __forceinline__ F div_fast(F a, F b) {
+    return make_float2(__fdividef(a.x, b.x), __fdividef(a.y, b.y));
   }
   static __device__ __forceinline__ F sqrt(F a) { return make_float2(__fsqrt_rn(a.x), __fsqrt_rn(a.y)); }
   static __device__ __forceinline__ F log(F a) { return make_float2(Ops1::log(a.x), Ops1::log(a.y)); }
