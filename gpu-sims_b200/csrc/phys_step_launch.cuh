@@ -11,7 +11,9 @@ namespace {
 // without Smagorinsky: 24 blocks (80 registers, up to ~100 bytes spilled in
 // the forced / moment-writing forms) against 20 (94 registers, no spills),
 // measured on B200: channel 512x128x128 39.3 vs 38.4 GLUPS, periodic TRT
-// 256^3 40.4 vs 37.7, lid cavity 192^3 38.8 vs 36.7.  With Smagorinsky the
+// 256^3 40.4 vs 37.7, lid cavity 192^3 38.8 vs 36.7; 28 blocks (72 registers,
+// 12-168 bytes spilled) fall back: 37.5 / 40.6 / 37.8 against 39.4 / 42.1 /
+// 38.1 on one box.  With Smagorinsky the
 // same bound spills 280-340 bytes and loses (128^3: 28.3 vs 32.8), so the
 // Smagorinsky forms have their own bound: fp32 20 blocks (128^3 / 256^3 BGK /
 // 256^3 TRT: 32.7 / 34.7 / 32.6 GLUPS against 30.2 / 31.7 / 31.0 at 16); fp16
